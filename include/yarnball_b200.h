@@ -1,0 +1,221 @@
+/*
+ * yarnball_b200.h - C ABI of the B200-native Stable Cosserat Rods substep.
+ *
+ * This is the boundary that replaces the static-library link to YarnBall::Sim
+ * (reference: KittenEngine/YarnBall/YarnBall.h:116-206).  Every entry point takes plain
+ * pointers and sizes, returns a yb_status and never calls exit(); the C++ drop-in header
+ * <yarnball/YarnBall.h> turns non-zero statuses back into std::runtime_error, as the
+ * reference does.
+ *
+ * Data model (identical to the reference's host side):
+ *   - a simulation owns host arrays verts (yb_vertex, 32 B each), qs (4 floats: x,y,z
+ *     bivector + w scalar), qRests (4 floats) and vels (3 floats), obtained with
+ *     yb_host_arrays(); the caller fills them, then configure/upload/download move data;
+ *   - parameters live in yb_meta, the non-pointer part of YarnBall::MetaData.
+ * A simulation may hold several independent scenes packed in one flat vertex array
+ * (yb_create_batch); scenes never collide with each other and each has its own yb_meta
+ * material parameters, while all of them advance with one time step.
+ *
+ * Threading: a yb_sim is not thread-safe; calls on one yb_sim are stream-ordered on its
+ * own CUDA stream.
+ */
+#ifndef YARNBALL_B200_H
+#define YARNBALL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum yb_status {
+    YB_OK = 0,
+    YB_ERR_INVALID_ARGUMENT = 1,
+    YB_ERR_TOO_FEW_VERTICES = 2,       /* Sim::Sim, YarnBall.cu:12 */
+    YB_ERR_NOT_CONFIGURED = 3,         /* setKStretch/setKBend before configure, YarnBall.cu:203,213 */
+    YB_ERR_DANGLING_SEGMENT = 4,       /* configure, YarnBall.cu:115-116 */
+    YB_ERR_ZERO_LENGTH_SEGMENT = 5,    /* configure, YarnBall.cu:128-129 */
+    YB_ERR_DETECTION_SCALER = 6,       /* uploadMeta, YarnBall.cu:230-231 */
+    YB_ERR_SEGMENT_TOO_SHORT = 7,      /* uploadMeta, YarnBall.cu:233-234 */
+    YB_ERR_MAX_COLLISIONS_PER_SEGMENT_EXCEEDED = 8, /* checkErrors, YarnBall.cu:283-286 */
+    YB_ERR_CUDA = 9,                   /* replaces checkCudaErrors' exit(), Common.h:15-21 */
+    YB_ERR_OUT_OF_MEMORY = 10,
+    YB_ERR_INTERNAL = 11,              /* a bounded device wait expired or the BVH stack overflowed */
+    YB_ERR_ALREADY_CONFIGURED = 12
+} yb_status;
+
+/* VertexFlags, YarnBall.h:34-40 */
+enum {
+    YB_HAS_PREV = 1,
+    YB_HAS_NEXT = 2,
+    YB_HAS_NEXT_ORIENTATION = 4,
+    YB_FIX_ORIENTATION = 8,
+    YB_COLLIDING = 16
+};
+
+/* Sim::ERROR_* / WARNING_*, YarnBall.h:118-122 */
+enum {
+    YB_ERROR_NONE = 0,
+    YB_ERROR_MAX_COLLISIONS_PER_SEGMENT_EXCEEDED = 1,
+    YB_WARNING_SEGMENT_INTERPENETRATION = 2
+};
+
+#define YB_MAX_COLLISIONS_PER_SEGMENT 128 /* YarnBall.h:20 */
+
+/* Vertex, YarnBall.h:52-61 (same field order and size: 32 bytes). */
+typedef struct yb_vertex {
+    float pos[3];
+    float invMass;
+    float lRest;
+    float kStretch;
+    int32_t connectionIndex;
+    uint32_t flags;
+} yb_vertex;
+
+/* MetaData without its device pointers, YarnBall.h:63-114 (same field order). */
+typedef struct yb_meta {
+    float gravity[3];
+    int32_t numItr;
+    float worldFloorNormal[3];
+    float worldFloorPos;
+    float h;
+    float lastH;
+    float time;
+    int32_t numVerts;
+    float damping;
+    float drag;
+    float frictionCoeff;
+    float kCollision;
+    float kFriction;
+    float detectionRadius;
+    float scaledDetectionRadius;
+    float radius;
+    float accelerationRatio;
+    float barrierThickness;
+    float detectionScaler;
+    float bvhRebuildPeriod;
+    int32_t detectionPeriod;
+    float maxSegLen;
+    float minSegLen;
+    int32_t useStepSizeLimit;
+    int32_t useVelocityRadius;
+} yb_meta;
+
+typedef struct yb_sim yb_sim;
+
+enum { YB_PRECISION_FP32 = 0, YB_PRECISION_FP64 = 1 };
+
+/* Sim::Sim(int numVerts), YarnBall.cu:11-51: defaults for meta and every vertex. */
+yb_status yb_create(int32_t numVerts, yb_sim** out);
+
+/* Several scenes in one flat array (no reference counterpart; the batched form).
+ * Scene s owns vertices [sum(vertsPerScene[0..s)), +vertsPerScene[s]).  precision is
+ * YB_PRECISION_FP32 (production) or YB_PRECISION_FP64 (the FP64 build of the same kernels). */
+yb_status yb_create_batch(int32_t numScenes, const int32_t* vertsPerScene, int32_t precision, yb_sim** out);
+
+/* Sim::~Sim, YarnBall.cu:53-85. */
+void yb_destroy(yb_sim* sim);
+
+/* Host arrays Sim::verts/qs/qRests/vels, YarnBall.h:124-127.  Owned by the simulation
+ * (page-locked when a GPU is present); valid until yb_destroy. */
+yb_status yb_host_arrays(yb_sim* sim, yb_vertex** verts, float** qs, float** qRests, float** vels);
+
+/* Sim::meta, YarnBall.h:129.  scene selects the scene of a batch (0 for a plain Sim). */
+yb_status yb_get_meta(yb_sim* sim, int32_t scene, yb_meta* out);
+yb_status yb_set_meta(yb_sim* sim, int32_t scene, const yb_meta* in);
+
+/* Sim::maxH, YarnBall.h:130. */
+yb_status yb_get_max_h(yb_sim* sim, float* maxH);
+yb_status yb_set_max_h(yb_sim* sim, float maxH);
+
+/* Sim::configure(float density), YarnBall.cu:91-200: flags, rest lengths, masses, frames,
+ * rest Darboux rotors, device allocation, uploadMeta and upload.  Applies to every scene. */
+yb_status yb_configure(yb_sim* sim, float density);
+
+/* Sim::setKStretch / Sim::setKBend, YarnBall.cu:202-224 (host arrays only, like the
+ * reference; call yb_upload afterwards).  scene < 0 applies to all scenes. */
+yb_status yb_set_kstretch(yb_sim* sim, int32_t scene, float k);
+yb_status yb_set_kbend(yb_sim* sim, int32_t scene, float k);
+
+/* Sim::upload / download / zeroVelocities, YarnBall.cu:247-274 (blocking, like the reference). */
+yb_status yb_upload(yb_sim* sim);
+yb_status yb_download(yb_sim* sim);
+yb_status yb_zero_velocities(yb_sim* sim);
+
+/* Sim::advance(float h), step.cpp:101-120: ceil(dt/maxH) substeps, then the error check.
+ * *advanced receives dt (the reference declares float but returns nothing). */
+yb_status yb_advance(yb_sim* sim, float dt, float* advanced);
+
+/* Sim::step(float), step.cpp:122-124: one advance(maxH). */
+yb_status yb_step(yb_sim* sim, float dt);
+
+/* Sim::stepCount, YarnBall.h:163. */
+yb_status yb_step_count(yb_sim* sim, uint64_t* out);
+
+/* Sim::bounds, YarnBall.cu:87-89: root box of the BVH (padded segment boxes) after the
+ * last detection; minmax = {min x,y,z, max x,y,z}.  scene < 0 gives the union. */
+yb_status yb_bounds(yb_sim* sim, int32_t scene, float minmax[6]);
+
+/* Sim::printCollisionStats, statistics.cpp:5-23, returned instead of printed:
+ * unordered contact pairs, segments with at least one contact, largest list. */
+yb_status yb_collision_stats(yb_sim* sim, uint64_t* totalPairs, int32_t* segmentsWithContacts,
+                             int32_t* maxPerSegment);
+
+/* Sim::lastErrorCode / lastWarningCode, YarnBall.h:134-135. */
+yb_status yb_last_error(yb_sim* sim, int32_t* errorCode, int32_t* warningCode);
+
+/* Sim::initialInvMasses, YarnBall.h:131 (filled by configure). */
+yb_status yb_initial_inv_masses(yb_sim* sim, const float** out, int32_t* count);
+
+/* Human-readable text of a status (replaces the reference's fprintf messages). */
+const char* yb_status_string(yb_status s);
+
+/* ---- Additions without a reference counterpart ---------------------------------- */
+
+/* Engine tuning: Newton block size (64/128/256/512) and whether substeps replay captured
+ * CUDA graphs.  Defaults come from the autotuner or 256 / graphs on. */
+yb_status yb_set_tuning(yb_sim* sim, int32_t iterBlock, int32_t useGraphs);
+yb_status yb_get_tuning(yb_sim* sim, int32_t* iterBlock, int32_t* useGraphs);
+
+/* Kernels launched on the device so far (each graph node counts once per replay). */
+yb_status yb_launch_count(yb_sim* sim, uint64_t* out);
+
+/* Number of vertices, scenes and precision of a simulation. */
+yb_status yb_info(yb_sim* sim, int32_t* numVerts, int32_t* numScenes, int32_t* precision);
+
+/* Contacts with centre-line distance <= 2 * radius seen since creation (interpenetrations). */
+yb_status yb_penetration_count(yb_sim* sim, int64_t* out);
+
+/* FP64 diagnostics of the current device state (substep start), computed on the device:
+ * out[0] kinetic, out[1] gravity potential, out[2] stretch, out[3] bend, out[4] barrier
+ * energy (each contact pair once), out[5] max |v|, out[6] min normalised contact gap,
+ * out[7] contact pairs.  Energies follow the definitions written beside the kernel. */
+yb_status yb_diagnostics(yb_sim* sim, double out[8]);
+
+/* State access in the simulation's precision widened to double (for accuracy studies):
+ * pos (3n), vel (3n), q (4n); any pointer may be NULL. */
+yb_status yb_read_state_f64(yb_sim* sim, double* pos, double* vel, double* q);
+
+/* Device-side debugging views used by the parity tests (copies to host buffers):
+ *   numCols (n int32), cols (n*128 int32, column-major seg + n*k), stepLimit (n float),
+ *   dx (4n in state precision widened to double).  NULL pointers are skipped. */
+yb_status yb_debug_contacts(yb_sim* sim, int32_t* numCols, int32_t* cols, float* stepLimit);
+yb_status yb_debug_dx(yb_sim* sim, double* dx4);
+
+/* Runs only the substep phases selected by mask on the current device state:
+ * 1 = predictor (initItr), 2 = detection with BVH rebuild, 4 = detection with refit only,
+ * 8 = step limit, 16 = one Newton+orientation iteration, 32 = advection (endItr).
+ * Meant for phase-by-phase parity tests; advance() is the production path. */
+yb_status yb_debug_phases(yb_sim* sim, int32_t mask, float h);
+
+/* Stable radix sort of (key, value) pairs on host buffers through the device sort used by
+ * the BVH build (ascending by the low `bits` key bits). */
+yb_status yb_debug_sort_pairs(const uint64_t* keys, const int32_t* vals, int32_t n, int32_t bits,
+                              uint64_t* keysOut, int32_t* valsOut);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* YARNBALL_B200_H */

@@ -1,0 +1,181 @@
+"""CPU oracle bindings (test infrastructure only).
+
+Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as the checker; never
+by the product.  The oracle is a C++/OpenMP restatement of the reference's substep
+(oracle/yb_oracle.cpp).  PARITY UNPINNED: the reference cannot be built or run here and has
+no golden vectors for this path; see yb_oracle.h.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libyb_oracle.so")
+
+FP64, FP32, FP32_MIXED = 0, 1, 2
+
+_d = ctypes.POINTER(ctypes.c_double)
+_f = ctypes.POINTER(ctypes.c_float)
+_i = ctypes.POINTER(ctypes.c_int32)
+_v = ctypes.c_void_p
+
+_SIG = {
+    "orc_configure": (ctypes.c_int, [ctypes.c_int, ctypes.c_float, _v, _f, _f, _f, _f, _f]),
+    "orc_set_kstretch": (None, [ctypes.c_int, _v, ctypes.c_float]),
+    "orc_set_kbend": (None, [ctypes.c_int, _v, _f, ctypes.c_float]),
+    "orc_upload_meta": (ctypes.c_int, [_v]),
+    "orc_create": (_v, [ctypes.c_int, ctypes.c_int]),
+    "orc_destroy": (None, [_v]),
+    "orc_set_state": (None, [_v, _v, _f, _f, _f, _i, ctypes.c_int, _v]),
+    "orc_set_meta": (None, [_v, ctypes.c_int, _v]),
+    "orc_set_last_vel": (None, [_v, _d]),
+    "orc_set_schedule": (None, [_v, ctypes.c_uint64]),
+    "orc_advance": (ctypes.c_int, [_v, ctypes.c_float, ctypes.c_float]),
+    "orc_phases": (ctypes.c_int, [_v, ctypes.c_int, ctypes.c_float]),
+    "orc_get_state": (None, [_v, _d, _d, _d, _d, _d]),
+    "orc_get_contacts": (None, [_v, _i, _i, _d]),
+    "orc_diagnostics": (None, [_v, _d]),
+    "orc_penetrations": (ctypes.c_int64, [_v]),
+    "orc_set_threads": (None, [ctypes.c_int]),
+    "orc_max_threads": (ctypes.c_int, []),
+}
+
+_LIB = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def load():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIG.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = lib
+    return _LIB
+
+
+def _p(a, t):
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(ctypes.POINTER(t))
+
+
+def meta_bytes(meta_struct):
+    """The engine's YbMeta and the oracle's orc_meta share one layout."""
+    return ctypes.string_at(ctypes.addressof(meta_struct), ctypes.sizeof(meta_struct))
+
+
+def configure(verts, qs, qRests, density=1e-3):
+    """Host setup (YarnBall.cu:91-157) on copies; returns (status, verts, qs, qRests, invMass0, maxSeg, minSeg)."""
+    lib = load()
+    v = np.ascontiguousarray(verts.copy())
+    q = np.ascontiguousarray(np.array(qs, np.float32, copy=True))
+    qr = np.ascontiguousarray(np.array(qRests, np.float32, copy=True))
+    im = np.zeros(len(v), np.float32)
+    mx, mn = ctypes.c_float(), ctypes.c_float()
+    st = lib.orc_configure(len(v), density, v.ctypes.data, _p(q, ctypes.c_float), _p(qr, ctypes.c_float),
+                           _p(im, ctypes.c_float), ctypes.byref(mx), ctypes.byref(mn))
+    return st, v, q, qr, im, mx.value, mn.value
+
+
+def set_kstretch(verts, k):
+    load().orc_set_kstretch(len(verts), verts.ctypes.data, k)
+
+
+def set_kbend(verts, qRests, k):
+    load().orc_set_kbend(len(verts), verts.ctypes.data, _p(qRests, ctypes.c_float), k)
+
+
+def set_threads(t):
+    load().orc_set_threads(int(t))
+
+
+def max_threads():
+    return int(load().orc_max_threads())
+
+
+class OracleSim:
+    """State + substep of the restated algorithm (FP64, FP32 or FP32 with the engine's policy)."""
+
+    def __init__(self, verts, vels, qs, qRests, metas, mode=FP64, scene_of=None, last_vel=None, step_counter=0):
+        self.lib = load()
+        n = len(verts)
+        self.n = n
+        self.h = self.lib.orc_create(n, mode)
+        v = np.ascontiguousarray(verts)
+        vel = np.ascontiguousarray(vels, dtype=np.float32)
+        q = np.ascontiguousarray(qs, dtype=np.float32)
+        qr = np.ascontiguousarray(qRests, dtype=np.float32)
+        mb = b"".join(meta_bytes(m) for m in metas)
+        mbuf = ctypes.create_string_buffer(mb, len(mb))
+        so = None
+        if scene_of is not None:
+            so = np.ascontiguousarray(scene_of, dtype=np.int32)
+        self.lib.orc_set_state(self.h, v.ctypes.data, _p(vel, ctypes.c_float), _p(q, ctypes.c_float),
+                               _p(qr, ctypes.c_float), _p(so, ctypes.c_int32) if so is not None else None,
+                               len(metas), ctypes.cast(mbuf, ctypes.c_void_p))
+        if last_vel is not None:
+            lv = np.ascontiguousarray(last_vel, dtype=np.float64)
+            self.lib.orc_set_last_vel(self.h, _p(lv, ctypes.c_double))
+        if step_counter:
+            self.lib.orc_set_schedule(self.h, int(step_counter))
+
+    def close(self):
+        if self.h:
+            self.lib.orc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def advance(self, dt, maxH=1e-3):
+        return self.lib.orc_advance(self.h, float(dt), float(maxH))
+
+    def phases(self, mask, h=0.0):
+        return self.lib.orc_phases(self.h, int(mask), float(h))
+
+    def state(self):
+        n = self.n
+        pos = np.zeros((n, 3)); vel = np.zeros((n, 3)); q = np.zeros((n, 4)); dx = np.zeros((n, 4)); lv = np.zeros((n, 3))
+        self.lib.orc_get_state(self.h, _p(pos, ctypes.c_double), _p(vel, ctypes.c_double), _p(q, ctypes.c_double),
+                               _p(dx, ctypes.c_double), _p(lv, ctypes.c_double))
+        return dict(pos=pos, vel=vel, q=q, dx=dx[:, :3].copy(), lastVel=lv)
+
+    def contacts(self):
+        n = self.n
+        nc = np.zeros(n, np.int32)
+        cols = np.zeros(n * 128, np.int32)
+        sl = np.zeros(n, np.float64)
+        self.lib.orc_get_contacts(self.h, _p(nc, ctypes.c_int32), _p(cols, ctypes.c_int32), _p(sl, ctypes.c_double))
+        lists = [cols[i + n * np.arange(nc[i])].copy() for i in range(n)]
+        return nc, lists, sl
+
+    def diagnostics(self):
+        out = np.zeros(8)
+        self.lib.orc_diagnostics(self.h, _p(out, ctypes.c_double))
+        keys = ["kinetic", "gravity", "stretch", "bend", "barrier", "max_speed", "min_gap", "pairs"]
+        return dict(zip(keys, out.tolist()))
+
+    def penetrations(self):
+        return int(self.lib.orc_penetrations(self.h))
+
+
+def from_sim(sim, mode=FP64, **kw):
+    """Oracle state from a yarnball_b200 Sim's host arrays and parameters (after configure)."""
+    metas = [sim.scene_meta(s).as_struct() for s in range(sim.numScenes)]
+    scene_of = None
+    if sim.numScenes > 1:
+        scene_of = np.repeat(np.arange(sim.numScenes, dtype=np.int32), np.diff(sim.sceneOffsets))
+    return OracleSim(sim.verts.copy(), sim.vels.copy(), sim.qs.copy(), sim.qRests.copy(), metas, mode=mode,
+                     scene_of=scene_of, **kw)

@@ -1,0 +1,145 @@
+"""GPU parity: the CUDA engine (through the C ABI) against the CPU oracle.
+
+Tolerances (stated here, used below):
+  * positions after one substep: max |x_gpu - x_fp64| <= 1e-5 x segment length
+  * orientations after one substep: max angle(q_gpu, q_fp64) <= 1e-5 rad
+  * after one frame (34 substeps): relative error <= 1e-4, measured as
+    max_i |x_gpu - x_fp64| / max_i |x_fp64 - x_start|  (error relative to the motion)
+  * contact lists and step limits after detection: bit-exact against the FP32 oracle that
+    follows the engine's precision policy (same positions and predictor output)
+  * FP64 build against the FP64 oracle: 1e-9 x segment length
+"""
+import numpy as np
+import pytest
+
+import oracle
+import yarnball_b200 as yb
+from yarnball_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+SEG = 2e-3
+H = 1.0 / 1020.0
+
+
+def quat_angle(q1, q2):
+    q1 = q1 / np.linalg.norm(q1, axis=1, keepdims=True)
+    q2 = q2 / np.linalg.norm(q2, axis=1, keepdims=True)
+    s = np.sign(np.sum(q1 * q2, axis=1, keepdims=True))
+    s[s == 0] = 1
+    a = np.linalg.norm(q1 - s * q2, axis=1)
+    b = np.linalg.norm(q1 + s * q2, axis=1)
+    return 2 * np.arctan2(a, b)
+
+
+def seg_rows(sim):
+    return (sim.verts["flags"] & 2) != 0
+
+
+def test_sort_matches_stable_argsort():
+    rng = np.random.default_rng(3)
+    for n, bits in [(1, 30), (7, 30), (2048, 30), (2049, 39), (100003, 39), (300000, 64)]:
+        keys = rng.integers(0, 2**min(bits, 63), size=n, dtype=np.uint64)
+        keys[: n // 3] = keys[0]  # many duplicates: stability matters
+        vals = np.arange(n, dtype=np.int32)
+        ko, vo = yb.sort_pairs(keys, vals, bits)
+        order = np.argsort(keys, kind="stable")
+        assert np.array_equal(ko, keys[order]), (n, bits)
+        assert np.array_equal(vo, vals[order]), (n, bits)
+
+
+def test_readme_one_substep_vs_fp64():
+    sim = scenes.build_readme()
+    orc = oracle.from_sim(sim, mode=oracle.FP64)
+    sim.advance(1e-3)  # exactly one substep
+    orc.advance(1e-3, 1e-3)
+    pos, vel, q = sim.read_state_f64()
+    ref = orc.state()
+    perr = np.abs(pos - ref["pos"]).max()
+    assert perr <= 1e-5 * SEG, perr
+    qerr = quat_angle(q[seg_rows(sim)], ref["q"][seg_rows(sim)]).max()
+    assert qerr <= 1e-5, qerr
+
+
+def test_readme_one_frame_rel_err():
+    sim = scenes.build_readme()
+    x0 = sim.verts["pos"].astype(np.float64).copy()
+    orc = oracle.from_sim(sim, mode=oracle.FP64)
+    for _ in range(3):
+        sim.advance(1 / 30.0)
+        orc.advance(1 / 30.0, 1e-3)
+    pos, _, q = sim.read_state_f64()
+    ref = orc.state()
+    rel = np.abs(pos - ref["pos"]).max() / np.abs(ref["pos"] - x0).max()
+    assert rel <= 1e-4, rel
+
+
+def test_readme_fp64_build_vs_fp64_oracle():
+    sim = scenes.build_readme(precision="fp64")
+    orc = oracle.from_sim(sim, mode=oracle.FP64)
+    sim.advance(1 / 30.0)
+    orc.advance(1 / 30.0, 1e-3)
+    pos, _, q = sim.read_state_f64()
+    ref = orc.state()
+    assert np.abs(pos - ref["pos"]).max() <= 1e-9 * SEG
+    assert quat_angle(q[seg_rows(sim)], ref["q"][seg_rows(sim)]).max() <= 1e-9
+
+
+def _compare_detection(sim, orc):
+    """Predictor + detection on both sides from identical state; lists and limits bit-exact."""
+    sim.debug_phases(1 | 2, H)
+    orc.phases(1 | 2, H)
+    nc_g, lists_g, sl_g = sim.debug_contacts()
+    nc_o, lists_o, sl_o = orc.contacts()
+    # the predictor output feeds the filter: it must agree bit for bit first
+    dx_g = sim.debug_dx()
+    dx_o = orc.state()["dx"]
+    assert np.array_equal(dx_g.astype(np.float32), dx_o.astype(np.float32))
+    assert np.array_equal(nc_g, nc_o)
+    for i in np.nonzero(nc_g)[0]:
+        assert np.array_equal(lists_g[i], lists_o[i]), i
+    segs = seg_rows(sim)
+    assert np.array_equal(sl_g[segs], sl_o[segs].astype(np.float32))
+    return int(nc_g.sum())
+
+
+def test_pile_small_pair_set_bit_exact():
+    sim = scenes.build_pile(seed=11, yarns=96, verts=64)
+    orc = oracle.from_sim(sim, mode=oracle.FP32_MIXED)
+    total = _compare_detection(sim, orc)
+    assert total > 0
+
+
+def test_pile_full_pair_set_bit_exact():
+    sim = scenes.build_pile(seed=1)
+    orc = oracle.from_sim(sim, mode=oracle.FP32_MIXED)
+    total = _compare_detection(sim, orc)
+    assert total > 100000
+
+
+def test_pile_small_substep_vs_fp64():
+    sim = scenes.build_pile(seed=5, yarns=64, verts=64)
+    orc = oracle.from_sim(sim, mode=oracle.FP64)
+    sim.advance(1e-3)
+    orc.advance(1e-3, 1e-3)
+    pos, _, q = sim.read_state_f64()
+    ref = orc.state()
+    perr = np.abs(pos - ref["pos"]).max()
+    assert perr <= 1e-5 * SEG, perr
+    qerr = quat_angle(q[seg_rows(sim)], ref["q"][seg_rows(sim)]).max()
+    assert qerr <= 1e-5, qerr
+
+
+def test_batched_equals_alone():
+    spec = scenes.batched_spec(seed=5, num_scenes=4, cap=40000)
+    batch, spec = scenes.build_batched(seed=5, spec=spec)
+    batch.advance(1 / 30.0)
+    pos_b, _, q_b = batch.read_state_f64()
+    for s in range(len(spec[0])):
+        alone = scenes.build_scene_alone(spec, s, seed=5)
+        alone.advance(1 / 30.0)
+        pos_a, _, q_a = alone.read_state_f64()
+        o0, o1 = batch.sceneOffsets[s], batch.sceneOffsets[s + 1]
+        assert np.array_equal(pos_b[o0:o1], pos_a), s
+        assert np.array_equal(q_b[o0:o1], q_a), s
+        alone.close()

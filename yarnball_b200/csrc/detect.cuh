@@ -1,0 +1,100 @@
+// detect.cuh - separately rounded detection predicates shared by the BVH and step kernels.
+//
+//   segment AABB        collision.cu:10-37   (buildAABBs, velocity radius included)
+//   narrow-phase keep   collision.cu:39-92   (buildCollisionList: glue/neighbour exemptions,
+//                                             closest points, d^2 < r^2)
+//   step-size limit     collision.cu:121-159 (recomputeStepLimitKernel)
+//
+// The pair test is always evaluated with the lower segment index as segment A, so both
+// segments of a pair reach the same decision and every contact list is symmetric.
+#pragma once
+#include "engine.cuh"
+
+namespace yb {
+
+template <typename R>
+struct Box {
+    R mn[3], mx[3];
+};
+
+// Padded AABB of segment k (k has hasNext).
+template <typename R>
+__device__ __forceinline__ Box<R> segment_box(const Dev<R>& d, int k, const SceneParams<R>& sp) {
+    typedef Ex<R> E;
+    const V4<R> p0 = d.pos[k];
+    const V4<R> p1 = d.pos[k + 1];
+    R pad = sp.sdr;
+    if (sp.useVelRadius) {
+        const R l0 = xlen2(xyz(d.dx[0][k]));
+        const R l1 = xlen2(xyz(d.dx[0][k + 1]));
+        pad = E::add(pad, E::sqrt(ymax(l0, l1)));
+    }
+    Box<R> b;
+    b.mn[0] = E::sub(ymin(p0.x, p1.x), pad);
+    b.mn[1] = E::sub(ymin(p0.y, p1.y), pad);
+    b.mn[2] = E::sub(ymin(p0.z, p1.z), pad);
+    b.mx[0] = E::add(ymax(p0.x, p1.x), pad);
+    b.mx[1] = E::add(ymax(p0.y, p1.y), pad);
+    b.mx[2] = E::add(ymax(p0.z, p1.z), pad);
+    return b;
+}
+
+// Closed-interval overlap of a query box with a stored box.
+template <typename R>
+__device__ __forceinline__ bool box_overlap(const Box<R>& q, const R* mn, const R* mx) {
+    return q.mn[0] <= mx[0] && mn[0] <= q.mx[0] && q.mn[1] <= mx[1] && mn[1] <= q.mx[1] && q.mn[2] <= mx[2] &&
+           mn[2] <= q.mx[2];
+}
+
+// Narrow-phase decision for segments x < y (both with hasNext, same scene).
+template <typename R>
+__device__ __forceinline__ bool pair_keep(const Dev<R>& d, int x, int y, const SceneParams<R>& sp) {
+    typedef Ex<R> E;
+    const int c0 = d.vp[x].cid;
+    const int c1 = d.vp[x + 1].cid;
+    if (c0 == y || c1 == y || c0 == y + 1 || c1 == y + 1) return false;
+    if (y - x <= 2) return false;
+    const V3<R> a0 = xyz(d.pos[x]);
+    const V3<R> a1 = xsub(xyz(d.pos[x + 1]), a0);
+    const V3<R> b0 = xsub(xyz(d.pos[y]), a0);
+    const V3<R> b1 = xsub(xyz(d.pos[y + 1]), a0);
+    const UVT<R> uv = closest_uv_exact(a1, b0, b1);
+    const V3<R> nrm = xsub(xscale(uv.u, a1), xmix(b0, b1, uv.v));
+    const R d2 = xlen2(nrm);
+    R r = E::mul(R(2), sp.sdr);
+    if (sp.useVelRadius) {
+        r = E::add(r, E::sqrt(ymax(xlen2(xyz(d.dx[0][x])), xlen2(xyz(d.dx[0][x + 1])))));
+        r = E::add(r, E::sqrt(ymax(xlen2(xyz(d.dx[0][y])), xlen2(xyz(d.dx[0][y + 1])))));
+    }
+    return d2 < E::mul(r, r);
+}
+
+// Step-size limit of segment k over its nc listed contacts.  Also counts contacts whose
+// centre-line distance is at or below 2 * radius (interpenetration), each unordered pair once.
+template <typename R>
+__device__ __forceinline__ R segment_step_limit(const Dev<R>& d, int k, const SceneParams<R>& sp, int nc) {
+    typedef Ex<R> E;
+    const V3<R> a0 = xyz(d.pos[k]);
+    const V3<R> a1 = xsub(xyz(d.pos[k + 1]), a0);
+    R m = sp.stepBase;
+    if (sp.useVelRadius) m = E::add(m, E::sqrt(xlen2(xyz(d.dx[0][k]))));
+    const R safe = E::mul(E::sub(R(1), R(0.1f)), R(0.5f));
+    int pen = 0;
+    for (int c = 0; c < nc; c++) {
+        const int o = d.cols[k + (size_t)d.n * c];
+        const V3<R> b0 = xsub(xyz(d.pos[o]), a0);
+        const V3<R> b1 = xsub(xyz(d.pos[o + 1]), a0);
+        const UVT<R> uv = closest_uv_exact(a1, b0, b1);
+        const V3<R> nrm = xsub(xscale(uv.u, a1), xmix(b0, b1, uv.v));
+        const R l = E::sqrt(xlen2(nrm));
+        m = ymin(m, E::mul(safe, l));
+        if (o > k && l <= sp.twoR) pen++;
+    }
+    if (pen) {
+        atomicAdd(&d.err[EW_PENETRATIONS], pen);
+        d.err[EW_WARNING] = 2;
+    }
+    return sp.useStepLimit ? m : yinf<R>();
+}
+
+}  // namespace yb

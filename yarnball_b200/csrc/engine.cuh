@@ -1,0 +1,120 @@
+// engine.cuh - device data layout and kernel entry points of the substep engine.
+//
+// Layout in HBM (structure of arrays, one element per vertex unless noted; R = float|double):
+//   pos      V4<R>  xyz = position at the start of the substep, w = invMass
+//   posC     V4<R>  Kahan compensation of pos (xyz), FP32 build only
+//   vel      V4<R>  xyz = velocity (kept intact during the iterations; y = h v + h^2 g is
+//                   formed on the fly instead of overwriting vel as YarnBall.cu does)
+//   lastVel  V4<R>  velocity of the previous substep (acceleration-aware initial guess)
+//   dx[2]    V4<R>  Newton iterate (double buffered: strict Jacobi)
+//   q[2]     V4<R>  segment orientation rotor (double buffered)
+//   qRest    V4<R>  rest Darboux rotor; its magnitude is the bending stiffness
+//   vp       VP<R>  {lRest, kStretch, connectionIndex, flags | scene << 8}
+//   stepLim  R      per-segment displacement limit (collision.cu:121-159)
+//   numCols  int    contacts of each segment
+//   cols     int    contact partner ids, column major: cols[seg + n * k], k < MAX_COLS
+// Segments are the vertices with hasNext; segs[] lists them and is the leaf set of the BVH.
+#pragma once
+#include "ybmath.cuh"
+
+namespace yb {
+
+constexpr int MAX_COLS = 128;  // MAX_COLLISIONS_PER_SEGMENT, YarnBall.h:20
+
+enum : uint32_t {
+    F_HAS_PREV = 1,
+    F_HAS_NEXT = 2,
+    F_HAS_NEXT_ORI = 4,
+    F_FIX_ORI = 8,
+    F_COLLIDING = 16,
+    F_USER_MASK = 0xFFu,
+};
+YB_HD int scene_of(uint32_t f) { return (int)(f >> 8); }
+
+// Error word slots (device int[8]).
+enum {
+    EW_ERROR = 0,        // 1 = max collisions per segment exceeded (collision.cu:81-90)
+    EW_WARNING = 1,      // 2 = segment interpenetration (YarnBall.h:121)
+    EW_INTERNAL = 2,     // bit mask of IE_* below
+    EW_PENETRATIONS = 3, // number of contacts seen with distance <= 2 * radius (cumulative)
+    EW_MAX_COLS = 4,     // largest contact count of any segment (cumulative max)
+    EW_COUNT = 8
+};
+enum { IE_BVH_STACK = 1, IE_SORT_WAIT = 2, IE_GRID_WAIT = 4, IE_REFIT = 8 };
+
+template <typename R>
+struct VP {
+    R lRest, kStretch;
+    int cid;
+    uint32_t flags;
+};
+
+template <typename R>
+struct SceneParams {
+    R h, lastH, invH, hh;           // h, previous h, 1/h, h*h
+    R gx, gy, gz, g2;               // gravity and |g|^2
+    R dragFactor;                   // 1 - drag * h
+    R D;                            // damping / h
+    R accel;                        // accelerationRatio
+    R twoR;                         // 2 * radius
+    R invb;                         // 1 / barrierThickness
+    R kCol;                         // kCollision / barrierThickness
+    R fricK, fricMu;                // kFriction, frictionCoeff
+    R sdr;                          // scaledDetectionRadius
+    R stepBase;                     // detectionRadius * (detectionScaler - 1)
+    int useStepLimit, useVelRadius;
+};
+
+template <typename R>
+struct BNode {                     // internal BVH node: boxes of both children + links
+    R lmin[3], lmax[3], rmin[3], rmax[3];
+    int left, right;               // child code: >= 0 internal node, < 0 leaf -(seg + 1)
+    int parent, pad;
+};
+
+template <typename R>
+struct Dev {
+    int n;            // vertices
+    int nseg;         // segments (= BVH leaves)
+    int numScenes;
+    V4<R>* pos;
+    V4<R>* posC;
+    V4<R>* vel;
+    V4<R>* lastVel;
+    V4<R>* dx[2];
+    V4<R>* q[2];
+    V4<R>* qRest;
+    VP<R>* vp;
+    R* stepLim;
+    int* numCols;
+    int* cols;
+    int* segs;        // segment -> vertex index, ascending (scene-contiguous)
+    const SceneParams<R>* sp;
+    int* err;         // EW_COUNT ints
+    // BVH
+    BNode<R>* nodes;  // nseg - 1 internal nodes
+    int* leafParent;  // per sorted leaf position
+    unsigned* refitCount;
+    int* sceneRoot;   // child code of each scene's subtree root (or INT_MIN when empty)
+    int* sceneSegOff; // numScenes + 1 prefix of segments per scene
+    unsigned long long* keys[2];
+    int* vals[2];
+    unsigned* sceneBox;   // 6 ordered-uint per scene: min xyz, max xyz of segment midpoints
+};
+
+// --- kernel launchers (stream-ordered; no host synchronisation) ---
+template <typename R> void launch_init(const Dev<R>& d, cudaStream_t s);
+template <typename R> void launch_end(const Dev<R>& d, int finalBuf, bool copyQ, bool kahan, cudaStream_t s);
+template <typename R> void launch_iter(const Dev<R>& d, int srcBuf, int block, cudaStream_t s);
+template <typename R> void launch_step_limit(const Dev<R>& d, cudaStream_t s);
+template <typename R> void launch_bvh_rebuild(const Dev<R>& d, cudaStream_t s, void* sortScratch, size_t sortScratchBytes, int keyBits);
+template <typename R> void launch_bvh_refit(const Dev<R>& d, cudaStream_t s);
+template <typename R> void launch_traverse(const Dev<R>& d, cudaStream_t s);
+template <typename R> void launch_bvh_reset(const Dev<R>& d, cudaStream_t s);  // scene roots := empty
+
+// Radix sort of (u64 key, int value) pairs, ascending by the low `bits` key bits, stable.
+// keys/vals ping-pong between [0] and [1]; the result lands in buffer (passes & 1).
+size_t radix_sort_scratch_bytes(int n);
+int radix_sort_pairs(unsigned long long* keys[2], int* vals[2], int n, int bits, void* scratch, int* err, cudaStream_t s);
+
+}  // namespace yb

@@ -1,0 +1,16 @@
+// io.cuh - launchers for layout conversion, diagnostics and BVH root boxes (k_io.cu).
+#pragma once
+#include "engine.cuh"
+
+namespace yb {
+template <typename R>
+void launch_convert_in(const Dev<R>& d, const void* hv, const float* hvel, const float* hq, const float* hqr,
+                       const int* sceneOf, cudaStream_t s);
+template <typename R> void launch_convert_out(const Dev<R>& d, void* hv, float* hvel, float* hq, cudaStream_t s);
+template <typename R> void launch_zero_vel(const Dev<R>& d, cudaStream_t s);
+template <typename R>
+void launch_state_f64(const Dev<R>& d, int buf, double* pos, double* vel, double* q, double* dx, cudaStream_t s);
+template <typename R> void launch_scene_root_box(const Dev<R>& d, float* out, cudaStream_t s);
+// Writes 8 doubles per block into part; returns the number of blocks.
+template <typename R> int launch_diag(const Dev<R>& d, double* part, cudaStream_t s);
+}  // namespace yb

@@ -1,0 +1,329 @@
+// k_bvh.cu - linear BVH over segment AABBs and the broadphase that emits contact lists.
+//
+// The reference calls an LBVH library whose source is not part of the reference project
+// (KittenEngine/KittenGpuLBVH is an empty submodule; call sites collision.cu:94-119).  This
+// is a new implementation of the published method:
+//   * leaf keys: 30-bit Morton code of the segment midpoint, normalised by its scene's
+//     bounds, with the scene id above bit 30 so that every scene is one subtree;
+//   * stable LSD radix sort of (key, segment) pairs (k_sort.cu);
+//   * Karras 2012 binary radix tree emission, one thread per internal node, ties between
+//     equal keys broken by leaf position;
+//   * bottom-up AABB refit with one atomic arrival counter per internal node;
+//   * traversal: every segment walks its own scene's subtree with its own padded box and
+//     keeps the partners that pass the narrow-phase filter (detect.cuh).  Each segment
+//     writes only its own list (no atomics on other segments' lists); the list is then
+//     sorted by partner id and the step-size limit is computed from it in the same thread.
+#include "detect.cuh"
+
+namespace yb {
+
+__device__ __forceinline__ unsigned f2ord(float f) {
+    unsigned u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float ord2f(unsigned u) {
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+template <typename R>
+__global__ void k_scene_box_init(Dev<R> d) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= d.numScenes) return;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        d.sceneBox[6 * s + a] = 0xFFFFFFFFu;
+        d.sceneBox[6 * s + 3 + a] = 0u;
+    }
+    d.sceneRoot[s] = INT_MIN;
+}
+
+// Per-scene bounds of segment midpoints (Morton normalisation).
+template <typename R>
+__global__ void __launch_bounds__(256) k_scene_bounds(Dev<R> d) {
+    const int si = blockIdx.x * blockDim.x + threadIdx.x;
+    if (si >= d.nseg) return;
+    const int k = d.segs[si];
+    const int sc = scene_of(d.vp[k].flags);
+    const V4<R> p0 = d.pos[k], p1 = d.pos[k + 1];
+    const float m[3] = {(float)((p0.x + p1.x) * R(0.5)), (float)((p0.y + p1.y) * R(0.5)),
+                        (float)((p0.z + p1.z) * R(0.5))};
+    // Warp-level pre-reduction when the whole warp belongs to one scene (the common case).
+    const unsigned mask = __activemask();
+    const int sc0 = __shfl_sync(mask, sc, __ffs(mask) - 1);
+    const bool uniform = __all_sync(mask, sc == sc0);
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        unsigned lo = f2ord(m[a]), hi = lo;
+        if (uniform) {
+            for (int o = 16; o > 0; o >>= 1) {
+                lo = min(lo, __shfl_xor_sync(mask, lo, o));
+                hi = max(hi, __shfl_xor_sync(mask, hi, o));
+            }
+            if ((threadIdx.x & 31) == (unsigned)(__ffs(mask) - 1)) {
+                atomicMin(&d.sceneBox[6 * sc + a], lo);
+                atomicMax(&d.sceneBox[6 * sc + 3 + a], hi);
+            }
+        } else {
+            atomicMin(&d.sceneBox[6 * sc + a], lo);
+            atomicMax(&d.sceneBox[6 * sc + 3 + a], hi);
+        }
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_morton(Dev<R> d) {
+    const int si = blockIdx.x * blockDim.x + threadIdx.x;
+    if (si >= d.nseg) return;
+    const int k = d.segs[si];
+    const int sc = scene_of(d.vp[k].flags);
+    const V4<R> p0 = d.pos[k], p1 = d.pos[k + 1];
+    const float m[3] = {(float)((p0.x + p1.x) * R(0.5)), (float)((p0.y + p1.y) * R(0.5)),
+                        (float)((p0.z + p1.z) * R(0.5))};
+    uint32_t code = 0;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const float lo = ord2f(d.sceneBox[6 * sc + a]);
+        const float hi = ord2f(d.sceneBox[6 * sc + 3 + a]);
+        const float ext = hi - lo;
+        float c = ext > 0.f ? (m[a] - lo) / ext : 0.5f;
+        int qv = (int)(c * 1024.f);
+        qv = qv < 0 ? 0 : (qv > 1023 ? 1023 : qv);
+        code |= morton_spread10((uint32_t)qv) << (2 - a);
+    }
+    d.keys[0][si] = ((unsigned long long)sc << 30) | code;
+    d.vals[0][si] = k;
+}
+
+__device__ __forceinline__ int kdelta(const unsigned long long* __restrict__ keys, int n, int i, int j) {
+    if (j < 0 || j >= n) return -1;
+    const unsigned long long a = keys[i], b = keys[j];
+    if (a == b) return 64 + __clz(i ^ j);
+    return __clzll(a ^ b);
+}
+
+// Karras 2012 internal-node emission + scene subtree roots.
+template <typename R>
+__global__ void __launch_bounds__(256) k_karras(Dev<R> d, const unsigned long long* __restrict__ keys,
+                                                const int* __restrict__ vals) {
+    const int n = d.nseg;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    // single-leaf scenes
+    {
+        const unsigned long long sc = keys[i] >> 30;
+        const bool lo = (i == 0) || ((keys[i - 1] >> 30) != sc);
+        const bool hi = (i == n - 1) || ((keys[i + 1] >> 30) != sc);
+        if (lo && hi) d.sceneRoot[sc] = -(vals[i] + 1);
+    }
+    if (i >= n - 1) return;
+    const int dir = (kdelta(keys, n, i, i + 1) - kdelta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
+    const int dmin = kdelta(keys, n, i, i - dir);
+    int lmax = 2;
+    while (kdelta(keys, n, i, i + lmax * dir) > dmin) lmax <<= 1;
+    int l = 0;
+    for (int t = lmax >> 1; t >= 1; t >>= 1)
+        if (kdelta(keys, n, i, i + (l + t) * dir) > dmin) l += t;
+    const int j = i + l * dir;
+    const int dnode = kdelta(keys, n, i, j);
+    int s = 0;
+    int t = l;
+    do {
+        t = (t + 1) >> 1;
+        if (kdelta(keys, n, i, i + (s + t) * dir) > dnode) s += t;
+    } while (t > 1);
+    const int gamma = i + s * dir + (dir < 0 ? -1 : 0);
+    const int first = min(i, j), last = max(i, j);
+    BNode<R>& nd = d.nodes[i];
+    if (first == gamma) {
+        nd.left = -(vals[gamma] + 1);
+        d.leafParent[gamma] = i;
+    } else {
+        nd.left = gamma;
+        d.nodes[gamma].parent = i;
+    }
+    if (last == gamma + 1) {
+        nd.right = -(vals[gamma + 1] + 1);
+        d.leafParent[gamma + 1] = i;
+    } else {
+        nd.right = gamma + 1;
+        d.nodes[gamma + 1].parent = i;
+    }
+    if (i == 0) nd.parent = -1;
+    const unsigned long long sc = keys[first] >> 30;
+    if ((keys[last] >> 30) == sc && (first == 0 || (keys[first - 1] >> 30) != sc) &&
+        (last == n - 1 || (keys[last + 1] >> 30) != sc))
+        d.sceneRoot[sc] = i;
+}
+
+template <typename R>
+__device__ __forceinline__ void store_child_box(BNode<R>& nd, bool left, const Box<R>& b) {
+    R* mn = left ? nd.lmin : nd.rmin;
+    R* mx = left ? nd.lmax : nd.rmax;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        __stcg(mn + a, b.mn[a]);
+        __stcg(mx + a, b.mx[a]);
+    }
+}
+
+// Bottom-up refit: leaf boxes from the current positions/velocity radius, unions upward.
+// refitCount must be zero on entry (cleared by the launcher).
+template <typename R>
+__global__ void __launch_bounds__(256) k_refit(Dev<R> d, const int* __restrict__ sortedVals) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= d.nseg) return;
+    const int k = sortedVals[p];
+    const SceneParams<R>& sp = d.sp[scene_of(d.vp[k].flags)];
+    Box<R> b = segment_box(d, k, sp);
+    int code = -(k + 1);
+    if (d.nseg == 1) return;
+    int node = d.leafParent[p];
+    int guard = 0;
+    while (node >= 0) {
+        if (node >= d.nseg - 1) {  // only a corrupt tree gets here: report, touch nothing
+            atomicOr(&d.err[EW_INTERNAL], IE_REFIT);
+            return;
+        }
+        BNode<R>& nd = d.nodes[node];
+        const bool isLeft = (nd.left == code);
+        store_child_box(nd, isLeft, b);
+        __threadfence();
+        const unsigned old = atomicAdd(&d.refitCount[node], 1u);
+        if (old == 0u) return;  // first arrival: the sibling finishes this node
+        __threadfence();
+        const R* omn = isLeft ? nd.rmin : nd.lmin;
+        const R* omx = isLeft ? nd.rmax : nd.lmax;
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            b.mn[a] = ymin(b.mn[a], __ldcg(omn + a));
+            b.mx[a] = ymax(b.mx[a], __ldcg(omx + a));
+        }
+        code = node;
+        node = nd.parent;
+        if (++guard > 4096) {  // a cycle would mean a corrupt tree: stop and report
+            atomicOr(&d.err[EW_INTERNAL], IE_REFIT);
+            return;
+        }
+    }
+}
+
+constexpr int BVH_STACK = 64;
+
+template <typename R>
+__global__ void __launch_bounds__(128) k_traverse(Dev<R> d) {
+    const int si = blockIdx.x * blockDim.x + threadIdx.x;
+    if (si >= d.nseg) return;
+    const int k = d.segs[si];
+    const uint32_t flags = d.vp[k].flags;
+    const int sc = scene_of(flags);
+    const SceneParams<R>& sp = d.sp[sc];
+    const Box<R> qb = segment_box(d, k, sp);
+    const size_t n = (size_t)d.n;
+    int* __restrict__ cl = d.cols + k;
+    int cnt = 0;
+    int node = d.sceneRoot[sc];
+    if (node >= 0) {
+        int stack[BVH_STACK];
+        int top = 0;
+        while (true) {
+            const BNode<R>& nd = d.nodes[node];
+            bool ol = box_overlap(qb, nd.lmin, nd.lmax);
+            bool orr = box_overlap(qb, nd.rmin, nd.rmax);
+            const int L = nd.left, Rc = nd.right;
+            if (ol && L < 0) {
+                const int j = -L - 1;
+                if (j != k && pair_keep(d, min(j, k), max(j, k), sp)) {
+                    if (cnt < MAX_COLS) cl[n * cnt] = j;
+                    cnt++;
+                }
+                ol = false;
+            }
+            if (orr && Rc < 0) {
+                const int j = -Rc - 1;
+                if (j != k && pair_keep(d, min(j, k), max(j, k), sp)) {
+                    if (cnt < MAX_COLS) cl[n * cnt] = j;
+                    cnt++;
+                }
+                orr = false;
+            }
+            if (ol && orr) {
+                if (top < BVH_STACK) {
+                    stack[top++] = Rc;
+                } else {
+                    atomicOr(&d.err[EW_INTERNAL], IE_BVH_STACK);
+                }
+                node = L;
+            } else if (ol) {
+                node = L;
+            } else if (orr) {
+                node = Rc;
+            } else {
+                if (top == 0) break;
+                node = stack[--top];
+            }
+        }
+    }
+    if (cnt > MAX_COLS) d.err[EW_ERROR] = 1;
+    const int nc = min(cnt, MAX_COLS);
+    if (nc) atomicMax(&d.err[EW_MAX_COLS], cnt);
+    // Insertion sort of the list by partner id (fixed summation order in the iteration).
+    for (int a = 1; a < nc; a++) {
+        const int v = cl[n * a];
+        int b = a - 1;
+        while (b >= 0 && cl[n * b] > v) {
+            cl[n * (b + 1)] = cl[n * b];
+            b--;
+        }
+        cl[n * (b + 1)] = v;
+    }
+    d.numCols[k] = nc;
+    d.stepLim[k] = segment_step_limit(d, k, sp, nc);
+}
+
+template <typename R>
+void launch_bvh_rebuild(const Dev<R>& d, cudaStream_t s, void* sortScratch, size_t, int keyBits) {
+    if (d.nseg <= 0) return;
+    const int nb = (d.nseg + 255) / 256;
+    k_scene_box_init<R><<<(d.numScenes + 127) / 128, 128, 0, s>>>(d);
+    k_scene_bounds<R><<<nb, 256, 0, s>>>(d);
+    k_morton<R><<<nb, 256, 0, s>>>(d);
+    unsigned long long* keys[2] = {d.keys[0], d.keys[1]};
+    int* vals[2] = {d.vals[0], d.vals[1]};
+    const int buf = radix_sort_pairs(keys, vals, d.nseg, keyBits, sortScratch, d.err + EW_INTERNAL, s);
+    // After sorting, buffer 0 must hold the sorted pairs (refit/karras read it).
+    if (buf != 0) {
+        cudaMemcpyAsync(d.keys[0], d.keys[1], sizeof(unsigned long long) * d.nseg, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(d.vals[0], d.vals[1], sizeof(int) * d.nseg, cudaMemcpyDeviceToDevice, s);
+    }
+    k_karras<R><<<nb, 256, 0, s>>>(d, d.keys[0], d.vals[0]);
+    launch_bvh_refit(d, s);
+}
+
+template <typename R>
+void launch_bvh_reset(const Dev<R>& d, cudaStream_t s) {
+    if (d.numScenes > 0) k_scene_box_init<R><<<(d.numScenes + 127) / 128, 128, 0, s>>>(d);
+}
+
+template <typename R>
+void launch_bvh_refit(const Dev<R>& d, cudaStream_t s) {
+    if (d.nseg <= 1) return;
+    cudaMemsetAsync(d.refitCount, 0, sizeof(unsigned) * (d.nseg - 1), s);
+    k_refit<R><<<(d.nseg + 255) / 256, 256, 0, s>>>(d, d.vals[0]);
+}
+
+template <typename R>
+void launch_traverse(const Dev<R>& d, cudaStream_t s) {
+    if (d.nseg <= 0) return;
+    k_traverse<R><<<(d.nseg + 127) / 128, 128, 0, s>>>(d);
+}
+
+template void launch_bvh_rebuild<float>(const Dev<float>&, cudaStream_t, void*, size_t, int);
+template void launch_bvh_rebuild<double>(const Dev<double>&, cudaStream_t, void*, size_t, int);
+template void launch_bvh_refit<float>(const Dev<float>&, cudaStream_t);
+template void launch_bvh_refit<double>(const Dev<double>&, cudaStream_t);
+template void launch_bvh_reset<float>(const Dev<float>&, cudaStream_t);
+template void launch_bvh_reset<double>(const Dev<double>&, cudaStream_t);
+template void launch_traverse<float>(const Dev<float>&, cudaStream_t);
+template void launch_traverse<double>(const Dev<double>&, cudaStream_t);
+
+}  // namespace yb

@@ -1,0 +1,187 @@
+// k_sort.cu - stable LSD radix sort of (u64 key, int value) pairs, one kernel per 8-bit
+// digit ("onesweep": Adinets & Merrill 2022).
+//
+//   1. one histogram kernel counts every digit of every pass in a single read of the keys;
+//   2. a one-block kernel turns the histograms into per-pass digit offsets;
+//   3. per pass, each CTA takes the next tile (2048 keys) from an atomic counter, ranks its
+//      keys per digit with warp match (stable: warp-striped order = input order), publishes its
+//      per-digit count, and resolves its global offset by decoupled look-back over the
+//      predecessors' published counts/prefixes, then scatters.
+// Tiles only wait on tiles that obtained a smaller index from the counter, i.e. that are
+// already running, so the look-back always completes; every wait is still bounded and a
+// timeout sets IE_SORT_WAIT in the error word instead of hanging.
+#include "engine.cuh"
+
+namespace yb {
+
+constexpr int SORT_THREADS = 256;
+constexpr int SORT_ITEMS = 8;
+constexpr int SORT_TILE = SORT_THREADS * SORT_ITEMS;
+constexpr int SORT_WARPS = SORT_THREADS / 32;
+constexpr int SORT_MAX_PASSES = 8;
+constexpr unsigned ST_AGG = 1u << 30;
+constexpr unsigned ST_PRE = 2u << 30;
+constexpr unsigned ST_CNT = (1u << 30) - 1;
+constexpr int SORT_SPIN_LIMIT = 1 << 22;
+
+static inline int sort_tiles(int n) { return (n + SORT_TILE - 1) / SORT_TILE; }
+
+size_t radix_sort_scratch_bytes(int n) {
+    const size_t tiles = (size_t)sort_tiles(n < 1 ? 1 : n);
+    return sizeof(unsigned) * (SORT_MAX_PASSES * 256 + SORT_MAX_PASSES + SORT_MAX_PASSES * tiles * 256);
+}
+
+__global__ void __launch_bounds__(SORT_THREADS) k_sort_hist(const unsigned long long* __restrict__ keys, int n,
+                                                            int passes, unsigned* __restrict__ hist) {
+    __shared__ unsigned sh[SORT_MAX_PASSES][256];
+    for (int i = threadIdx.x; i < SORT_MAX_PASSES * 256; i += blockDim.x) (&sh[0][0])[i] = 0u;
+    __syncthreads();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const unsigned long long k = keys[i];
+        for (int p = 0; p < passes; p++) atomicAdd(&sh[p][(unsigned)(k >> (8 * p)) & 255u], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) {
+        const unsigned v = (&sh[0][0])[i];
+        if (v) atomicAdd(&hist[i], v);
+    }
+}
+
+// Exclusive scan of each pass's 256 digit counts (in place).  One block of 256 threads.
+__global__ void __launch_bounds__(256) k_sort_scan(unsigned* __restrict__ hist, int passes) {
+    __shared__ unsigned warpSum[8];
+    const int d = threadIdx.x, lane = d & 31, w = d >> 5;
+    for (int p = 0; p < passes; p++) {
+        const unsigned v = hist[p * 256 + d];
+        unsigned x = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warpSum[w] = x;
+        __syncthreads();
+        unsigned off = 0;
+        for (int i = 0; i < w; i++) off += warpSum[i];
+        hist[p * 256 + d] = off + x - v;
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(SORT_THREADS) k_sort_pass(const unsigned long long* __restrict__ kin,
+                                                            const int* __restrict__ vin,
+                                                            unsigned long long* __restrict__ kout,
+                                                            int* __restrict__ vout, int n, int shift,
+                                                            const unsigned* __restrict__ digitOff,
+                                                            unsigned* status, unsigned* tileCounter, int* err) {
+    __shared__ unsigned sTile;
+    __shared__ unsigned sWarp[SORT_WARPS][256];
+    __shared__ unsigned sBase[256];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) sTile = atomicAdd(tileCounter, 1u);
+    for (int i = tid; i < SORT_WARPS * 256; i += SORT_THREADS) (&sWarp[0][0])[i] = 0u;
+    __syncthreads();
+    const int tile = (int)sTile;
+    const long long base = (long long)tile * SORT_TILE + (long long)warp * 32 * SORT_ITEMS;
+    const unsigned ltmask = (1u << lane) - 1u;
+
+    unsigned long long key[SORT_ITEMS];
+    int val[SORT_ITEMS];
+    unsigned rank[SORT_ITEMS];
+#pragma unroll
+    for (int i = 0; i < SORT_ITEMS; i++) {
+        const long long idx = base + i * 32 + lane;
+        const bool valid = idx < n;
+        key[i] = valid ? kin[idx] : 0ull;
+        val[i] = valid ? vin[idx] : 0;
+        const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+        rank[i] = 0;
+        if (valid) {
+            const unsigned dig = (unsigned)(key[i] >> shift) & 255u;
+            const unsigned peers = __match_any_sync(vmask, dig);
+            const unsigned cnt = sWarp[warp][dig];
+            rank[i] = cnt + __popc(peers & ltmask);
+            __syncwarp(vmask);
+            if (lane == __ffs(peers) - 1) sWarp[warp][dig] = cnt + __popc(peers);
+            __syncwarp(vmask);
+        }
+    }
+    __syncthreads();
+    {
+        const int d = tid;
+        unsigned run = 0;
+#pragma unroll
+        for (int w = 0; w < SORT_WARPS; w++) {
+            const unsigned c = sWarp[w][d];
+            sWarp[w][d] = run;
+            run += c;
+        }
+        volatile unsigned* st = status;
+        unsigned excl = 0;
+        if (tile == 0) {
+            st[d] = ST_PRE | run;
+        } else {
+            st[(size_t)tile * 256 + d] = ST_AGG | run;
+            int t = tile - 1;
+            bool timedOut = false;
+            while (t >= 0 && !timedOut) {
+                unsigned wv = st[(size_t)t * 256 + d];
+                int spins = 0;
+                while ((wv >> 30) == 0u) {
+                    if (++spins > SORT_SPIN_LIMIT) {
+                        timedOut = true;
+                        break;
+                    }
+                    __nanosleep(32);
+                    wv = st[(size_t)t * 256 + d];
+                }
+                if (timedOut) break;
+                excl += wv & ST_CNT;
+                if (wv & ST_PRE) break;
+                t--;
+            }
+            if (timedOut) atomicOr(err, IE_SORT_WAIT);
+            __threadfence();
+            st[(size_t)tile * 256 + d] = ST_PRE | (excl + run);
+        }
+        sBase[d] = digitOff[d] + excl;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < SORT_ITEMS; i++) {
+        const long long idx = base + i * 32 + lane;
+        if (idx < n) {
+            const unsigned dig = (unsigned)(key[i] >> shift) & 255u;
+            const unsigned pos = sBase[dig] + sWarp[warp][dig] + rank[i];
+            if (pos < (unsigned)n) {  // always true unless a look-back wait expired
+                kout[pos] = key[i];
+                vout[pos] = val[i];
+            } else {
+                atomicOr(err, IE_SORT_WAIT);
+            }
+        }
+    }
+}
+
+int radix_sort_pairs(unsigned long long* keys[2], int* vals[2], int n, int bits, void* scratch, int* err,
+                     cudaStream_t s) {
+    if (n <= 1 || bits <= 0) return 0;
+    const int passes = (bits + 7) / 8 > SORT_MAX_PASSES ? SORT_MAX_PASSES : (bits + 7) / 8;
+    const int tiles = sort_tiles(n);
+    unsigned* hist = (unsigned*)scratch;
+    unsigned* counters = hist + SORT_MAX_PASSES * 256;
+    unsigned* status = counters + SORT_MAX_PASSES;
+    cudaMemsetAsync(scratch, 0, sizeof(unsigned) * (SORT_MAX_PASSES * 256 + SORT_MAX_PASSES + (size_t)passes * tiles * 256), s);
+    int hb = (n + SORT_THREADS * 4 - 1) / (SORT_THREADS * 4);
+    if (hb > 148 * 8) hb = 148 * 8;
+    k_sort_hist<<<hb, SORT_THREADS, 0, s>>>(keys[0], n, passes, hist);
+    k_sort_scan<<<1, 256, 0, s>>>(hist, passes);
+    for (int p = 0; p < passes; p++) {
+        const int src = p & 1;
+        k_sort_pass<<<tiles, SORT_THREADS, 0, s>>>(keys[src], vals[src], keys[src ^ 1], vals[src ^ 1], n, 8 * p,
+                                                   hist + p * 256, status + (size_t)p * tiles * 256, counters + p,
+                                                   err);
+    }
+    return passes & 1;
+}
+
+}  // namespace yb

@@ -1,0 +1,343 @@
+// k_step.cu - predictor, fused block-Jacobi Newton + orientation iteration, advection,
+// and the per-segment step-size limit.
+//
+// Reference semantics (file:line in the reference project):
+//   initItr               KittenEngine/YarnBall/sim/iteration.cu:7-41
+//   cosseratItr           KittenEngine/YarnBall/sim/cosserat.cu:20-207
+//   quaternionLambdaItr   KittenEngine/YarnBall/sim/cosserat.cu:209-253
+//   endItr                KittenEngine/YarnBall/sim/iteration.cu:48-61
+//   recomputeStepLimit    KittenEngine/YarnBall/sim/collision.cu:121-159
+//
+// Deliberate differences from the reference, all in the direction of determinism:
+//   * strict Jacobi: iteration k reads only iteration k-1's dx and q (double buffers); the
+//     reference updates both in place while neighbouring threads read them.
+//   * one kernel per iteration does the position solve and the orientation update: a block
+//     owns B-2 vertices and recomputes one halo segment on each side, so the orientation of
+//     segment i sees the new dx of vertices i and i+1 without a second launch.
+//   * contact lists are sorted by partner id, so force sums have a fixed order.
+#include "detect.cuh"
+
+namespace yb {
+
+template <typename R>
+__device__ __forceinline__ const SceneParams<R>& scene_params(const Dev<R>& d, uint32_t flags) {
+    return d.sp[scene_of(flags)];
+}
+
+// ---------------------------------------------------------------------------------------
+// Predictor (iteration.cu:7-41).  Every operation separately rounded: dx0 feeds the
+// bit-exact collision filter through the velocity radius.
+template <typename R>
+__global__ void __launch_bounds__(256) k_init(Dev<R> d) {
+    typedef Ex<R> E;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.n) return;
+    const uint32_t flags = d.vp[i].flags;
+    const SceneParams<R>& sp = scene_params(d, flags);
+    const V4<R> vel4 = d.vel[i];
+    const V4<R> lv4 = d.lastVel[i];
+    d.lastVel[i] = vel4;
+    const R h = sp.h;
+    V3<R> v = xyz(vel4);
+    V3<R> dx = xscale(h, v);
+    if (d.pos[i].w != R(0)) {
+        const R g2 = sp.g2;
+        if (g2 > R(0)) {
+            const V3<R> g(sp.gx, sp.gy, sp.gz);
+            V3<R> a(E::div(E::sub(v.x, lv4.x), sp.lastH), E::div(E::sub(v.y, lv4.y), sp.lastH),
+                    E::div(E::sub(v.z, lv4.z), sp.lastH));
+            R s = yclamp(E::div(xdot(a, g), g2), R(0), R(1));
+            dx = xadd(dx, xscale(E::mul(E::mul(h, h), s), g));
+        }
+    }
+    d.dx[0][i] = v4(dx, R(0));
+}
+
+// ---------------------------------------------------------------------------------------
+// Advection (iteration.cu:48-61) with Kahan-compensated position accumulation (FP32 build).
+template <typename R>
+__global__ void __launch_bounds__(256) k_end(Dev<R> d, int fb, int copyQ, int kahan) {
+    typedef Ex<R> E;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.n) return;
+    const uint32_t flags = d.vp[i].flags;
+    const SceneParams<R>& sp = scene_params(d, flags);
+    const V4<R> dx = d.dx[fb][i];
+    V4<R> p = d.pos[i];
+    if (p.w != R(0)) {
+        V4<R> v;
+        v.x = dx.x * sp.invH * sp.dragFactor;
+        v.y = dx.y * sp.invH * sp.dragFactor;
+        v.z = dx.z * sp.invH * sp.dragFactor;
+        v.w = R(0);
+        d.vel[i] = v;
+    }
+    if (kahan) {
+        V4<R> c = d.posC[i];
+        R yx = E::sub(dx.x, c.x), yy = E::sub(dx.y, c.y), yz = E::sub(dx.z, c.z);
+        R tx = E::add(p.x, yx), ty = E::add(p.y, yy), tz = E::add(p.z, yz);
+        c.x = E::sub(E::sub(tx, p.x), yx);
+        c.y = E::sub(E::sub(ty, p.y), yy);
+        c.z = E::sub(E::sub(tz, p.z), yz);
+        p.x = tx; p.y = ty; p.z = tz;
+        d.posC[i] = c;
+    } else {
+        p.x += dx.x; p.y += dx.y; p.z += dx.z;
+    }
+    d.pos[i] = p;
+    if (copyQ) d.q[0][i] = d.q[1][i];
+}
+
+template <typename R>
+__global__ void __launch_bounds__(128) k_step_limit(Dev<R> d) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= d.n) return;
+    const uint32_t flags = d.vp[k].flags;
+    R m = yinf<R>();
+    if (flags & F_HAS_NEXT) m = segment_step_limit(d, k, scene_params(d, flags), d.numCols[k]);
+    d.stepLim[k] = m;
+}
+
+// ---------------------------------------------------------------------------------------
+// IPC log barrier E(d) = -kCollision (d-1)^2 ln d on the normalised gap d, clamped to 1e-3:
+// returns dH = E''(d) / b^2 and the force magnitude ff (cosserat.cu:114-125).  Below d=1e-2
+// the log and the reciprocals are evaluated in FP64.
+template <typename R>
+__device__ __forceinline__ void barrier_terms(R d, R kCol, R invb, R& dH, R& ff) {
+    if (sizeof(R) == 4 && d < R(1e-2)) {
+        const double dd = d;
+        const double invd = 1.0 / dd;
+        const double logd = log(dd);
+        dH = (R)((-3.0 + (2.0 + invd) * invd - 2.0 * logd) * (double)kCol * (double)invb);
+        ff = (R)(-(1.0 - dd) * (dd - 1.0 + 2.0 * dd * logd) * invd * (double)kCol);
+    } else {
+        const R invd = R(1) / d;
+        const R logd = ylog(d);
+        dH = (R(-3) + (R(2) + invd) * invd - R(2) * logd) * kCol * invb;
+        ff = -(R(1) - d) * (d - R(1) + R(2) * d * logd) * invd * kCol;
+    }
+}
+
+// Contact of segment (p0,p1) with segment (b0,b1) on the current iterate (cosserat.cu:92-148).
+// Accumulates into the forces/Hessians of the segment's two endpoints.
+template <typename R>
+__device__ __forceinline__ void contact_term(V3<R> p0, V3<R> p1, V3<R> dx0, V3<R> dx1, V3<R> b0, V3<R> b1,
+                                             V3<R> db0, V3<R> db1, const SceneParams<R>& sp, V3<R>& fa,
+                                             H3<R>& Ha, V3<R>& fb, H3<R>& Hb) {
+    const UVT<R> uv = closest_uv((p1 - p0) + (dx1 - dx0), (b0 - p0) + (db0 - dx0), (b1 - p0) + (db1 - dx0));
+    const V3<R> dpos = mix(p0, p1, uv.u) - mix(b0, b1, uv.v);
+    const V3<R> ddpos = mix(dx0, dx1, uv.u) - mix(db0, db1, uv.v);
+    V3<R> nrm = dpos + ddpos;
+    const R dist = len(nrm);
+    nrm *= R(1) / dist;
+    const R wb = uv.u;
+    const R wa = R(1) - uv.u;
+    R gap = (dist - sp.twoR) * sp.invb;
+    if (gap > R(1)) return;
+    gap = ymax(gap, R(1e-3f));
+    R dH, ff;
+    barrier_terms(gap, sp.kCol, sp.invb, dH, ff);
+    const R D = sp.D;
+    fa += (ff * wa - D * dH * wa * wa * dot(nrm, dx0)) * nrm;
+    fb += (ff * wb - D * dH * wb * wb * dot(nrm, dx1)) * nrm;
+    dH *= R(1) + D;
+    Ha.add_outer(nrm, dH * wa * wa);
+    Hb.add_outer(nrm, dH * wb * wb);
+    // Friction on the current iterate: tangential relative displacement.
+    const V3<R> u = ddpos - dot(nrm, ddpos) * nrm;
+    const R ul = len(u);
+    if (ul > R(0)) {
+        const R f1 = ymin(sp.fricK, sp.fricMu * ff / ul);
+        fa -= (f1 * wa) * u;
+        fb -= (f1 * wb) * u;
+        const R sa = wa * wa * f1, sb = wb * wb * f1;
+        Ha.add_diag(sa); Ha.add_outer(nrm, -sa);
+        Hb.add_diag(sb); Hb.add_outer(nrm, -sb);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// One block-Jacobi iteration: position solve (cosseratItr) then orientation update
+// (quaternionLambdaItr), strict Jacobi.  Block b handles vertices k = b*(B-2)-1+t,
+// t in [0,B): it writes vertices t in [1, B-2] and recomputes the halo t=0 and t=B-1.
+template <typename R, int B>
+__global__ void __launch_bounds__(B) k_iter(Dev<R> d, int src) {
+    constexpr int CORE = B - 2;
+    const int t = threadIdx.x;
+    const int k = blockIdx.x * CORE - 1 + t;
+    const int n = d.n;
+    const bool valid = (k >= 0) && (k < n);
+    const V4<R>* __restrict__ DX = d.dx[src];
+    const V4<R>* __restrict__ QO = d.q[src];
+
+    __shared__ R sFb[3][B];
+    __shared__ R sHb[6][B];
+    __shared__ R sSL[B];
+    __shared__ R sDX[3][B];
+
+    V3<R> fa(R(0)), fb(R(0));
+    H3<R> Ha, Hb;
+    Ha.zero(); Hb.zero();
+    R sl = yinf<R>();
+    uint32_t flags = 0;
+    R invMass = R(0), lRest = R(1), kStretch = R(0);
+    V3<R> p0(R(0)), p1(R(0)), dx(R(0)), dx1(R(0));
+    Q<R> q0 = qmk(R(0), R(0), R(0), R(1));
+    const SceneParams<R>* spp = d.sp;
+
+    if (valid) {
+        const VP<R> vp = d.vp[k];
+        flags = vp.flags;
+        lRest = vp.lRest;
+        kStretch = vp.kStretch;
+        spp = &d.sp[scene_of(flags)];
+        const SceneParams<R>& sp = *spp;
+        const V4<R> P = d.pos[k];
+        p0 = xyz(P);
+        invMass = P.w;
+        dx = xyz(DX[k]);
+        q0 = qof(QO[k]);
+        const R D = sp.D;
+        if (invMass != R(0)) {
+            // Inertia: H = m/h^2, f = m/h^2 (y - dx), y = h v + h^2 g (iteration.cu:26, cosserat.cu:40-45)
+            const V4<R> v = d.vel[k];
+            const R hh = sp.hh;
+            const V3<R> y(sp.h * v.x + hh * sp.gx, sp.h * v.y + hh * sp.gy, sp.h * v.z + hh * sp.gz);
+            Ha.diag(R(1) / (invMass * hh));
+            fa = (R(1) / (hh * invMass)) * (y - dx);
+        }
+        if (vp.cid >= 0) {
+            // Glue spring to the connected vertex (cosserat.cu:46-53)
+            const R stiff = R(40);
+            const V3<R> pc = xyz(d.pos[vp.cid]);
+            const V3<R> dc = xyz(DX[vp.cid]);
+            fa -= stiff * ((p0 - pc) + (dx - dc) + D * dx);
+            Ha.add_diag(stiff * (R(1) + D));
+        }
+        if (flags & F_HAS_NEXT) {
+            p1 = xyz(d.pos[k + 1]);
+            dx1 = xyz(DX[k + 1]);
+            sl = d.stepLim[k];
+            // Stretch-shear coupling to the segment orientation (cosserat.cu:63-81)
+            const R invl = R(1) / lRest;
+            const V3<R> c = ((p1 - p0) + (dx1 - dx)) * invl - qrotate(q0, V3<R>(R(1), R(0), R(0)));
+            const R ks = kStretch * invl;
+            R dd = ks * invl;
+            fa += ks * c - (D * dd) * dx;
+            fb += -ks * c - (D * dd) * dx1;
+            dd *= R(1) + D;
+            Ha.add_diag(dd);
+            Hb.add_diag(dd);
+            // Barrier + friction over the contact list
+            const int nc = d.numCols[k];
+            const int* __restrict__ cl = d.cols + k;
+            for (int c2 = 0; c2 < nc; c2++) {
+                const int j = __ldg(cl + (size_t)n * c2);
+                const V3<R> b0 = xyz(d.pos[j]);
+                const V3<R> b1 = xyz(d.pos[j + 1]);
+                const V3<R> db0 = xyz(DX[j]);
+                const V3<R> db1 = xyz(DX[j + 1]);
+                contact_term(p0, p1, dx, dx1, b0, b1, db0, db1, sp, fa, Ha, fb, Hb);
+            }
+        }
+    }
+    sFb[0][t] = fb.x; sFb[1][t] = fb.y; sFb[2][t] = fb.z;
+#pragma unroll
+    for (int e = 0; e < 6; e++) sHb[e][t] = Hb.d[e];
+    sSL[t] = sl;
+    __syncthreads();
+
+    // Vertex solve: own segment + previous segment's endpoint share (cosserat.cu:175-205)
+    V3<R> dxn = dx;
+    if (valid && t > 0) {
+        if (flags & F_HAS_PREV) {
+            fa += V3<R>(sFb[0][t - 1], sFb[1][t - 1], sFb[2][t - 1]);
+            H3<R> hp;
+#pragma unroll
+            for (int e = 0; e < 6; e++) hp.d[e] = sHb[e][t - 1];
+            Ha.add(hp);
+            sl = ymin(sl, sSL[t - 1]);
+        }
+        if (invMass != R(0)) {
+            dxn = dx + spp->accel * solve3(Ha, fa);
+            const R l = len(dxn);
+            if (l > sl && l > R(0)) dxn *= sl / l;
+        }
+    }
+    sDX[0][t] = dxn.x; sDX[1][t] = dxn.y; sDX[2][t] = dxn.z;
+    const bool core = valid && t >= 1 && t <= CORE;
+    if (core) d.dx[src ^ 1][k] = v4(dxn, R(0));
+    __syncthreads();
+
+    // Orientation update of segment k (cosserat.cu:209-253)
+    if (core) {
+        Q<R> qn = q0;
+        if (!(flags & F_FIX_ORI) && (flags & F_HAS_NEXT)) {
+            const V3<R> dxb(sDX[0][t + 1], sDX[1][t + 1], sDX[2][t + 1]);
+            V3<R> v = ((p1 - p0) + (dxb - dxn)) * (R(1) / lRest);
+            v *= R(-2) * kStretch;
+            Q<R> b = qmk(R(0), R(0), R(0), R(0));
+            if (flags & F_HAS_PREV) {
+                const Q<R> qr = qof(d.qRest[k - 1]);
+                const Q<R> qq = qof(QO[k - 1]);
+                const R s = qdot(qmul(qinv(qq), q0), qr) > R(0) ? R(1) : R(-1);
+                b = qadd(b, qscale(s, qmul(qq, qr)));
+            }
+            if (flags & F_HAS_NEXT_ORI) {
+                const Q<R> qr = qof(d.qRest[k]);
+                const Q<R> qq = qof(QO[k + 1]);
+                const R s = qdot(qmul(qinv(q0), qq), qr) > R(0) ? R(1) : R(-1);
+                b = qadd(b, qscale(s, qmul(qq, qinv(qr))));
+            }
+            const R lambda = len(v) + qlen(b);
+            const Q<R> vb1 = qmul(qmul(qmk(v, R(0)), b), qmk(R(1), R(0), R(0), R(0)));
+            qn = qnormalize(qadd(vb1, qscale(lambda, b)));
+        }
+        d.q[src ^ 1][k] = v4of(qn);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+template <typename R>
+void launch_init(const Dev<R>& d, cudaStream_t s) {
+    if (d.n <= 0) return;
+    k_init<R><<<(d.n + 255) / 256, 256, 0, s>>>(d);
+}
+
+template <typename R>
+void launch_end(const Dev<R>& d, int finalBuf, bool copyQ, bool kahan, cudaStream_t s) {
+    if (d.n <= 0) return;
+    k_end<R><<<(d.n + 255) / 256, 256, 0, s>>>(d, finalBuf, copyQ ? 1 : 0, kahan ? 1 : 0);
+}
+
+template <typename R>
+void launch_step_limit(const Dev<R>& d, cudaStream_t s) {
+    if (d.n <= 0) return;
+    k_step_limit<R><<<(d.n + 127) / 128, 128, 0, s>>>(d);
+}
+
+template <typename R>
+void launch_iter(const Dev<R>& d, int srcBuf, int block, cudaStream_t s) {
+    if (d.n <= 0) return;
+    // FP64 at 512 threads would exceed the 48 KB static shared-memory limit: use 256.
+    if (sizeof(R) == 8 && block == 512) block = 256;
+    switch (block) {
+        case 64: k_iter<R, 64><<<(d.n + 61) / 62, 64, 0, s>>>(d, srcBuf); break;
+        case 128: k_iter<R, 128><<<(d.n + 125) / 126, 128, 0, s>>>(d, srcBuf); break;
+        case 512:
+            if constexpr (sizeof(R) == 4) k_iter<R, 512><<<(d.n + 509) / 510, 512, 0, s>>>(d, srcBuf);
+            break;
+        default: k_iter<R, 256><<<(d.n + 253) / 254, 256, 0, s>>>(d, srcBuf); break;
+    }
+}
+
+template void launch_init<float>(const Dev<float>&, cudaStream_t);
+template void launch_init<double>(const Dev<double>&, cudaStream_t);
+template void launch_end<float>(const Dev<float>&, int, bool, bool, cudaStream_t);
+template void launch_end<double>(const Dev<double>&, int, bool, bool, cudaStream_t);
+template void launch_step_limit<float>(const Dev<float>&, cudaStream_t);
+template void launch_step_limit<double>(const Dev<double>&, cudaStream_t);
+template void launch_iter<float>(const Dev<float>&, int, int, cudaStream_t);
+template void launch_iter<double>(const Dev<double>&, int, int, cudaStream_t);
+
+}  // namespace yb

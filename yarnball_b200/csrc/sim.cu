@@ -1,0 +1,1033 @@
+// sim.cu - host side of the substep engine and the C ABI (include/yarnball_b200.h).
+//
+// Reference interfaces replaced here (KittenEngine/YarnBall/...):
+//   Sim::Sim / ~Sim                     YarnBall.cu:11-85
+//   Sim::configure                      YarnBall.cu:91-200
+//   Sim::setKStretch / setKBend         YarnBall.cu:202-224
+//   Sim::uploadMeta                     YarnBall.cu:226-237
+//   Sim::upload / download / zeroVel    YarnBall.cu:239-274
+//   Sim::checkErrors                    YarnBall.cu:276-304
+//   Sim::rebuildCUDAGraph / advance     sim/step.cpp:5-59
+//   Sim::detectCollisions               sim/collision.cu:94-119
+//   Sim::printCollisionStats            sim/statistics.cpp:5-23
+//
+// One substep on the device is: predictor -> [detection: BVH rebuild or refit, traversal
+// (+ step limit)] or [step limit] -> numItr fused Newton/orientation iterations ->
+// advection.  No step reads anything back to the host (the reference's BVH query returns
+// its pair count to the host every detection); each of the three substep shapes is captured
+// once as a CUDA graph and replayed.
+#include <cmath>
+#include <cfloat>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "yarnball_b200.h"
+#include "engine.cuh"
+#include "io.cuh"
+
+using namespace yb;
+
+namespace {
+
+constexpr int GRAPH_TYPES = 3;  // 0: detect + rebuild, 1: detect + refit, 2: no detection
+
+struct EngineBase {
+    virtual ~EngineBase() {}
+    virtual yb_status upload() = 0;
+    virtual yb_status download() = 0;
+    virtual yb_status zero_vel() = 0;
+    virtual void write_params() = 0;
+    virtual uint64_t enqueue_substep(bool detect, bool rebuild) = 0;
+    virtual yb_status run_substep(int type) = 0;
+    virtual void invalidate_graphs() = 0;
+    virtual yb_status check_errors() = 0;
+    virtual yb_status read_state_f64(double* pos, double* vel, double* q, double* dx, int buf) = 0;
+    virtual yb_status contacts(int* numCols, int* cols, float* stepLimit) = 0;
+    virtual yb_status bounds(int scene, float* out) = 0;
+    virtual yb_status diagnostics(double* out) = 0;
+    virtual uint64_t debug_phases(int mask, int& buf) = 0;
+    virtual int64_t penetrations() = 0;
+};
+
+}  // namespace
+
+struct yb_sim {
+    int n = 0;
+    int numScenes = 1;
+    int precision = YB_PRECISION_FP32;
+    std::vector<int> sceneOff;  // numScenes + 1
+    std::vector<yb_meta> meta;  // per scene
+    float maxH = 1e-3f;
+    yb_vertex* verts = nullptr;
+    float* qs = nullptr;
+    float* qRests = nullptr;
+    float* vels = nullptr;
+    bool pinned = false;
+    std::vector<float> initialInvMasses;
+    bool configured = false;
+    float lastBVHRebuild = INFINITY;
+    uint64_t stepCounter = 0;
+    int lastErrorCode = 0, lastWarningCode = 0;
+    int iterBlock = 256;
+    int useGraphs = 1;
+    uint64_t launches = 0;
+    cudaStream_t stream = nullptr;
+    EngineBase* eng = nullptr;
+    int dbgBuf = 0;
+    std::vector<int> segs;  // host copy of the segment list
+};
+
+namespace {
+
+inline bool has(uint32_t f, uint32_t bit) { return (f & bit) != 0; }
+inline uint32_t setf(uint32_t f, uint32_t bit, bool on) { return on ? (f | bit) : (f & ~bit); }
+
+yb_status cuda_status(cudaError_t e) {
+    if (e == cudaSuccess) return YB_OK;
+    if (e == cudaErrorMemoryAllocation) return YB_ERR_OUT_OF_MEMORY;
+    return YB_ERR_CUDA;
+}
+#define YB_CUDA(x)                                     \
+    do {                                               \
+        cudaError_t e_ = (x);                          \
+        if (e_ != cudaSuccess) return cuda_status(e_); \
+    } while (0)
+
+void default_meta(yb_meta& m, int n, float maxH) {
+    // Sim::Sim, YarnBall.cu:14-35
+    std::memset(&m, 0, sizeof(m));
+    m.numVerts = n;
+    m.gravity[0] = 0.f; m.gravity[1] = -9.8f; m.gravity[2] = 0.f;
+    m.h = maxH;
+    m.drag = 0.2f;
+    m.damping = 1e-6f;
+    m.time = 0.f;
+    m.radius = 1e-4f;
+    m.barrierThickness = 8e-4f;
+    m.accelerationRatio = 1.f;
+    m.kCollision = 1e-5f;
+    m.detectionScaler = 1.2f;
+    m.frictionCoeff = 0.1f;
+    m.kFriction = 5.f;
+    m.detectionPeriod = 1;
+    m.useStepSizeLimit = 1;
+    m.useVelocityRadius = 1;
+    m.bvhRebuildPeriod = 1 / 10.f;
+    m.numItr = 8;
+}
+
+// ---- host rotor helpers for configure (FP32, separately rounded: -ffp-contract=off) ----
+struct HQ { float x, y, z, w; };
+inline HQ hq_mul(HQ l, HQ r) {
+    // Rotor.h:185-188
+    const float cx = l.y * r.z - r.y * l.z, cy = l.z * r.x - r.z * l.x, cz = l.x * r.y - r.x * l.y;
+    HQ o;
+    o.x = l.w * r.x + r.w * l.x + cx;
+    o.y = l.w * r.y + r.w * l.y + cy;
+    o.z = l.w * r.z + r.w * l.z + cz;
+    o.w = l.w * r.w - (l.x * r.x + l.y * r.y + l.z * r.z);
+    return o;
+}
+inline HQ hq_inv(HQ q) { return HQ{-q.x, -q.y, -q.z, q.w}; }
+inline float hq_len(HQ q) { return std::sqrt(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w); }
+inline HQ hq_normalize(HQ q) {
+    const float s = 1.f / hq_len(q);
+    return HQ{q.x * s, q.y * s, q.z * s, q.w * s};
+}
+// Rotor::fromTo(from, to), Rotor.h:57-64, with orthoBasisX (Common.h:235-251) for opposite vectors.
+inline HQ hq_from_to(const float f[3], const float t[3]) {
+    float h[3] = {(f[0] + t[0]) * 0.5f, (f[1] + t[1]) * 0.5f, (f[2] + t[2]) * 0.5f};
+    const float l = h[0] * h[0] + h[1] * h[1] + h[2] * h[2];
+    if (l > 0) {
+        const float s = 1.f / std::sqrt(l);
+        h[0] *= s; h[1] *= s; h[2] *= s;
+    } else {
+        const float* nn = f;
+        if (nn[2] >= nn[1]) {
+            const float a = 1.0f / (1.0f + nn[2]);
+            const float b = -nn[0] * nn[1] * a;
+            h[0] = b; h[1] = 1.0f - nn[1] * nn[1] * a; h[2] = -nn[1];
+        } else {
+            const float a = 1.0f / (1.0f + nn[1]);
+            const float b = -nn[0] * nn[2] * a;
+            h[0] = 1.0f - nn[0] * nn[0] * a; h[1] = -nn[0]; h[2] = b;
+        }
+    }
+    HQ o;
+    o.x = f[1] * h[2] - h[1] * f[2];
+    o.y = f[2] * h[0] - h[2] * f[0];
+    o.z = f[0] * h[1] - h[0] * f[1];
+    o.w = f[0] * h[0] + f[1] * h[1] + f[2] * h[2];
+    return o;
+}
+
+// Sim::configure host part for one scene's vertex range, YarnBall.cu:91-157.
+yb_status configure_scene(yb_sim* S, int o, int m, float density, float& maxSeg, float& minSeg) {
+    yb_vertex* V = S->verts + o;
+    float* qs = S->qs + 4 * (size_t)o;
+    float* qr = S->qRests + 4 * (size_t)o;
+    maxSeg = 0.f;
+    minSeg = FLT_MAX;
+    // The last vertex of a scene cannot start a segment (the reference leaves this to the
+    // caller; a stray hasNext there would read past the scene).
+    V[m - 1].flags &= ~(uint32_t)(YB_HAS_NEXT | YB_HAS_NEXT_ORIENTATION);
+    V[0].flags &= ~(uint32_t)YB_HAS_PREV;
+    HQ lastQ{0.f, 0.f, 0.f, 1.f};
+    for (int i = 0; i < m; i++) {
+        yb_vertex& v = V[i];
+        if (i < m - 1) {
+            const bool hasNext = has(v.flags, YB_HAS_NEXT);
+            V[i + 1].flags = setf(V[i + 1].flags, YB_HAS_PREV, hasNext);
+            const bool hasNextNext = hasNext && has(V[i + 1].flags, YB_HAS_NEXT);
+            v.flags = setf(v.flags, YB_HAS_NEXT_ORIENTATION, hasNextNext);
+            if (!hasNext) v.flags |= (uint32_t)YB_FIX_ORIENTATION;
+        }
+        if (!has(v.flags, YB_HAS_PREV) && !has(v.flags, YB_HAS_NEXT)) return YB_ERR_DANGLING_SEGMENT;
+        v.lRest = 1.f / m;
+        float mass = 0;
+        if (has(v.flags, YB_HAS_PREV)) mass += V[i - 1].lRest;
+        if (has(v.flags, YB_HAS_NEXT)) {
+            const yb_vertex& v1 = V[i + 1];
+            const float seg[3] = {v1.pos[0] - v.pos[0], v1.pos[1] - v.pos[1], v1.pos[2] - v.pos[2]};
+            v.lRest = std::sqrt(seg[0] * seg[0] + seg[1] * seg[1] + seg[2] * seg[2]);
+            if (v.lRest == 0 || !std::isfinite(v.lRest)) return YB_ERR_ZERO_LENGTH_SEGMENT;
+            const float inv = 1.f / std::sqrt(seg[0] * seg[0] + seg[1] * seg[1] + seg[2] * seg[2]);
+            const float dir[3] = {seg[0] * inv, seg[1] * inv, seg[2] * inv};
+            const float e1[3] = {1.f, 0.f, 0.f};
+            const HQ qq = hq_from_to(e1, dir);
+            HQ t = hq_mul(hq_inv(qq), lastQ);
+            t = hq_normalize(HQ{t.x, 0.f, 0.f, t.w});
+            lastQ = hq_mul(qq, t);
+            mass += v.lRest;
+            maxSeg = std::max(maxSeg, v.lRest);
+            minSeg = std::min(minSeg, v.lRest);
+        }
+        qs[4 * i] = lastQ.x; qs[4 * i + 1] = lastQ.y; qs[4 * i + 2] = lastQ.z; qs[4 * i + 3] = lastQ.w;
+        mass *= 0.5f * density;
+        if (mass != 0)
+            v.invMass *= 1 / mass;
+        else
+            v.invMass = 0;
+        S->initialInvMasses[o + i] = v.invMass;
+    }
+    for (int i = 0; i < m - 1; i++) {
+        const HQ a{qs[4 * i], qs[4 * i + 1], qs[4 * i + 2], qs[4 * i + 3]};
+        const HQ b{qs[4 * i + 4], qs[4 * i + 5], qs[4 * i + 6], qs[4 * i + 7]};
+        const HQ r{qr[4 * i], qr[4 * i + 1], qr[4 * i + 2], qr[4 * i + 3]};
+        const float l = hq_len(r);
+        const HQ d = hq_mul(hq_inv(a), b);
+        qr[4 * i] = l * d.x; qr[4 * i + 1] = l * d.y; qr[4 * i + 2] = l * d.z; qr[4 * i + 3] = l * d.w;
+    }
+    return YB_OK;
+}
+
+// uploadMeta's derived radii and validation, YarnBall.cu:226-234.
+yb_status upload_meta_checks(yb_meta& m) {
+    m.detectionRadius = m.radius + 0.5f * m.barrierThickness;
+    m.scaledDetectionRadius = m.detectionRadius * m.detectionScaler;
+    if (m.detectionScaler <= 1) return YB_ERR_DETECTION_SCALER;
+    if (2 * m.minSegLen < 2 * m.radius + m.barrierThickness) return YB_ERR_SEGMENT_TOO_SHORT;
+    return YB_OK;
+}
+
+template <typename R>
+SceneParams<R> scene_params_of(const yb_meta& m) {
+    SceneParams<R> p;
+    std::memset(&p, 0, sizeof(p));
+    const R h = (R)m.h;
+    p.h = h;
+    p.lastH = (R)m.lastH;
+    p.invH = R(1) / h;
+    p.hh = h * h;
+    p.gx = (R)m.gravity[0]; p.gy = (R)m.gravity[1]; p.gz = (R)m.gravity[2];
+    p.g2 = (p.gx * p.gx + p.gy * p.gy) + p.gz * p.gz;
+    p.dragFactor = R(1) - (R)m.drag * h;
+    p.D = (R)m.damping / h;
+    p.accel = (R)m.accelerationRatio;
+    p.twoR = R(2) * (R)m.radius;
+    p.invb = R(1) / (R)m.barrierThickness;
+    p.kCol = (R)m.kCollision * p.invb;
+    p.fricK = (R)m.kFriction;
+    p.fricMu = (R)m.frictionCoeff;
+    const R dr = (R)m.radius + R(0.5f) * (R)m.barrierThickness;
+    p.sdr = dr * (R)m.detectionScaler;
+    p.stepBase = dr * ((R)m.detectionScaler - R(1));
+    p.useStepLimit = m.useStepSizeLimit ? 1 : 0;
+    p.useVelRadius = m.useVelocityRadius ? 1 : 0;
+    return p;
+}
+
+int scene_bits(int numScenes) {
+    int b = 0;
+    while ((1 << b) < numScenes) b++;
+    return b;
+}
+
+template <typename R>
+struct Engine : EngineBase {
+    yb_sim* S;
+    Dev<R> d{};
+    void* block = nullptr;  // one device allocation, sub-allocated
+    void* sortScratch = nullptr;
+    size_t sortBytes = 0;
+    int* sceneOf = nullptr;
+    char* stage = nullptr;  // host-layout staging: verts | vels | qs | qRests
+    float* rootBoxes = nullptr;
+    double* diagPart = nullptr;
+    SceneParams<R>* spDev = nullptr;
+    SceneParams<R>* spHost = nullptr;
+    int* errHost = nullptr;
+    cudaGraphExec_t graphs[GRAPH_TYPES] = {nullptr, nullptr, nullptr};
+    uint64_t graphLaunches[GRAPH_TYPES] = {0, 0, 0};
+    int graphItr = -1, graphBlock = -1, graphNseg = -1;
+    int keyBits = 30;
+    int64_t penTotal = 0;
+
+    explicit Engine(yb_sim* s) : S(s) {}
+
+    ~Engine() override {
+        for (auto& g : graphs)
+            if (g) cudaGraphExecDestroy(g);
+        if (block) cudaFree(block);
+        if (spHost) cudaFreeHost(spHost);
+        if (errHost) cudaFreeHost(errHost);
+    }
+
+    yb_status alloc() {
+        const size_t n = (size_t)S->n;
+        const size_t ns = (size_t)S->numScenes;
+        const size_t nn = n > 1 ? n - 1 : 1;
+        sortBytes = radix_sort_scratch_bytes((int)n);
+        size_t off = 0;
+        std::vector<std::pair<void**, size_t>> req;
+        auto want = [&](void** p, size_t bytes) { req.push_back({p, bytes}); };
+        want((void**)&d.pos, sizeof(V4<R>) * n);
+        want((void**)&d.posC, sizeof(V4<R>) * n);
+        want((void**)&d.vel, sizeof(V4<R>) * n);
+        want((void**)&d.lastVel, sizeof(V4<R>) * n);
+        want((void**)&d.dx[0], sizeof(V4<R>) * n);
+        want((void**)&d.dx[1], sizeof(V4<R>) * n);
+        want((void**)&d.q[0], sizeof(V4<R>) * n);
+        want((void**)&d.q[1], sizeof(V4<R>) * n);
+        want((void**)&d.qRest, sizeof(V4<R>) * n);
+        want((void**)&d.vp, sizeof(VP<R>) * n);
+        want((void**)&d.stepLim, sizeof(R) * n);
+        want((void**)&d.numCols, sizeof(int) * n);
+        want((void**)&d.cols, sizeof(int) * n * MAX_COLS);
+        want((void**)&d.segs, sizeof(int) * n);
+        want((void**)&spDev, sizeof(SceneParams<R>) * ns);
+        want((void**)&d.err, sizeof(int) * EW_COUNT);
+        want((void**)&d.nodes, sizeof(BNode<R>) * nn);
+        want((void**)&d.leafParent, sizeof(int) * n);
+        want((void**)&d.refitCount, sizeof(unsigned) * nn);
+        want((void**)&d.sceneRoot, sizeof(int) * ns);
+        want((void**)&d.keys[0], sizeof(unsigned long long) * n);
+        want((void**)&d.keys[1], sizeof(unsigned long long) * n);
+        want((void**)&d.vals[0], sizeof(int) * n);
+        want((void**)&d.vals[1], sizeof(int) * n);
+        want((void**)&d.sceneBox, sizeof(unsigned) * 6 * ns);
+        want((void**)&sortScratch, sortBytes);
+        want((void**)&sceneOf, sizeof(int) * n);
+        want((void**)&stage, (sizeof(yb_vertex) + 12 + 16 + 16) * n);
+        want((void**)&rootBoxes, sizeof(float) * 6 * ns);
+        want((void**)&diagPart, sizeof(double) * 8 * ((n + 255) / 256 + 1));
+        for (auto& r : req) off += (r.second + 255) & ~(size_t)255;
+        YB_CUDA(cudaMalloc(&block, off));
+        off = 0;
+        for (auto& r : req) {
+            *r.first = (char*)block + off;
+            off += (r.second + 255) & ~(size_t)255;
+        }
+        d.n = S->n;
+        d.numScenes = S->numScenes;
+        d.nseg = 0;
+        d.sp = spDev;
+        d.sceneSegOff = nullptr;
+        YB_CUDA(cudaHostAlloc((void**)&spHost, sizeof(SceneParams<R>) * ns, cudaHostAllocDefault));
+        YB_CUDA(cudaHostAlloc((void**)&errHost, sizeof(int) * EW_COUNT, cudaHostAllocDefault));
+        YB_CUDA(cudaMemsetAsync(d.err, 0, sizeof(int) * EW_COUNT, S->stream));
+        YB_CUDA(cudaMemsetAsync(d.numCols, 0, sizeof(int) * n, S->stream));
+        YB_CUDA(cudaMemsetAsync(d.lastVel, 0, sizeof(V4<R>) * n, S->stream));
+        YB_CUDA(cudaMemsetAsync(d.refitCount, 0, sizeof(unsigned) * nn, S->stream));
+        std::vector<int> so(n);
+        for (int s = 0; s < S->numScenes; s++)
+            for (int i = S->sceneOff[s]; i < S->sceneOff[s + 1]; i++) so[i] = s;
+        YB_CUDA(cudaMemcpyAsync(sceneOf, so.data(), sizeof(int) * n, cudaMemcpyHostToDevice, S->stream));
+        launch_bvh_reset(d, S->stream);
+        keyBits = 30 + scene_bits(S->numScenes);
+        YB_CUDA(cudaStreamSynchronize(S->stream));
+        return YB_OK;
+    }
+
+    yb_status upload() override {
+        const size_t n = (size_t)S->n;
+        // Segment list and connection validation from the host flags.
+        std::vector<int> segs;
+        segs.reserve(n);
+        for (int s = 0; s < S->numScenes; s++) {
+            for (int i = S->sceneOff[s]; i < S->sceneOff[s + 1]; i++) {
+                const int c = S->verts[i].connectionIndex;
+                if (c >= S->n || c < -1) return YB_ERR_INVALID_ARGUMENT;
+                if (i + 1 < S->sceneOff[s + 1] && has(S->verts[i].flags, YB_HAS_NEXT)) segs.push_back(i);
+            }
+        }
+        char* sv = stage;
+        char* svel = sv + sizeof(yb_vertex) * n;
+        char* sq = svel + 12 * n;
+        char* sqr = sq + 16 * n;
+        cudaStream_t st = S->stream;
+        YB_CUDA(cudaMemcpyAsync(sv, S->verts, sizeof(yb_vertex) * n, cudaMemcpyHostToDevice, st));
+        YB_CUDA(cudaMemcpyAsync(svel, S->vels, 12 * n, cudaMemcpyHostToDevice, st));
+        YB_CUDA(cudaMemcpyAsync(sq, S->qs, 16 * n, cudaMemcpyHostToDevice, st));
+        YB_CUDA(cudaMemcpyAsync(sqr, S->qRests, 16 * n, cudaMemcpyHostToDevice, st));
+        if (!segs.empty())
+            YB_CUDA(cudaMemcpyAsync(d.segs, segs.data(), sizeof(int) * segs.size(), cudaMemcpyHostToDevice, st));
+        launch_convert_in(d, sv, (const float*)svel, (const float*)sq, (const float*)sqr, sceneOf, st);
+        S->launches++;
+        YB_CUDA(cudaGetLastError());
+        YB_CUDA(cudaStreamSynchronize(st));
+        if ((int)segs.size() != d.nseg || segs != S->segs) {
+            d.nseg = (int)segs.size();
+            S->segs.swap(segs);
+            S->lastBVHRebuild = INFINITY;  // topology must be rebuilt
+            invalidate_graphs();
+        }
+        return YB_OK;
+    }
+
+    yb_status download() override {
+        const size_t n = (size_t)S->n;
+        char* sv = stage;
+        char* svel = sv + sizeof(yb_vertex) * n;
+        char* sq = svel + 12 * n;
+        cudaStream_t st = S->stream;
+        launch_convert_out(d, sv, (float*)svel, (float*)sq, st);
+        S->launches++;
+        YB_CUDA(cudaGetLastError());
+        YB_CUDA(cudaMemcpyAsync(S->verts, sv, sizeof(yb_vertex) * n, cudaMemcpyDeviceToHost, st));
+        YB_CUDA(cudaMemcpyAsync(S->vels, svel, 12 * n, cudaMemcpyDeviceToHost, st));
+        YB_CUDA(cudaMemcpyAsync(S->qs, sq, 16 * n, cudaMemcpyDeviceToHost, st));
+        YB_CUDA(cudaStreamSynchronize(st));
+        return YB_OK;
+    }
+
+    yb_status zero_vel() override {
+        launch_zero_vel(d, S->stream);
+        S->launches++;
+        YB_CUDA(cudaGetLastError());
+        return YB_OK;
+    }
+
+    void write_params() override {
+        for (int s = 0; s < S->numScenes; s++) spHost[s] = scene_params_of<R>(S->meta[s]);
+        cudaMemcpyAsync(spDev, spHost, sizeof(SceneParams<R>) * S->numScenes, cudaMemcpyHostToDevice, S->stream);
+    }
+
+    int num_itr() const {
+        int it = 0;
+        for (const auto& m : S->meta) it = std::max(it, (int)m.numItr);
+        return it;
+    }
+
+    // Enqueues one substep on the stream; returns the number of kernels it launches.
+    uint64_t enqueue_substep(bool detect, bool rebuild) override {
+        cudaStream_t st = S->stream;
+        uint64_t k = 0;
+        launch_init(d, st); k++;
+        if (detect && d.nseg > 0) {
+            if (rebuild) {
+                launch_bvh_rebuild(d, st, sortScratch, sortBytes, keyBits);
+                const int passes = d.nseg > 1 ? (keyBits + 7) / 8 : 0;
+                k += 3 + (d.nseg > 1 ? 2 + passes : 0) + 1 + (d.nseg > 1 ? 1 : 0);
+            } else {
+                launch_bvh_refit(d, st);
+                k += d.nseg > 1 ? 1 : 0;
+            }
+            launch_traverse(d, st); k++;
+        } else {
+            launch_step_limit(d, st); k++;
+        }
+        const int I = num_itr();
+        for (int it = 0; it < I; it++) {
+            launch_iter(d, it & 1, S->iterBlock, st);
+            k++;
+        }
+        launch_end(d, I & 1, (I & 1) != 0, sizeof(R) == 4, st); k++;
+        return k;
+    }
+
+    void invalidate_graphs() override {
+        for (auto& g : graphs) {
+            if (g) cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+        graphItr = graphBlock = graphNseg = -1;
+    }
+
+    yb_status run_substep(int type) override {
+        const bool detect = type != 2, rebuild = type == 0;
+        if (!S->useGraphs) {
+            S->launches += enqueue_substep(detect, rebuild);
+            YB_CUDA(cudaGetLastError());
+            return YB_OK;
+        }
+        if (graphItr != num_itr() || graphBlock != S->iterBlock || graphNseg != d.nseg) {
+            invalidate_graphs();
+            graphItr = num_itr();
+            graphBlock = S->iterBlock;
+            graphNseg = d.nseg;
+        }
+        if (!graphs[type]) {
+            cudaGraph_t g = nullptr;
+            YB_CUDA(cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal));
+            graphLaunches[type] = enqueue_substep(detect, rebuild);
+            cudaError_t e = cudaStreamEndCapture(S->stream, &g);
+            if (e != cudaSuccess) return cuda_status(e);
+            e = cudaGraphInstantiate(&graphs[type], g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) {
+                graphs[type] = nullptr;
+                return cuda_status(e);
+            }
+        }
+        YB_CUDA(cudaGraphLaunch(graphs[type], S->stream));
+        S->launches += graphLaunches[type];
+        return YB_OK;
+    }
+
+    yb_status check_errors() override {
+        YB_CUDA(cudaGetLastError());
+        YB_CUDA(cudaMemcpyAsync(errHost, d.err, sizeof(int) * EW_COUNT, cudaMemcpyDeviceToHost, S->stream));
+        YB_CUDA(cudaStreamSynchronize(S->stream));
+        yb_status st = YB_OK;
+        penTotal = errHost[EW_PENETRATIONS];
+        if (errHost[EW_ERROR] != 0) {
+            S->lastErrorCode = errHost[EW_ERROR];
+            st = YB_ERR_MAX_COLLISIONS_PER_SEGMENT_EXCEEDED;
+        }
+        if (errHost[EW_WARNING] != 0) S->lastWarningCode = errHost[EW_WARNING];
+        if (errHost[EW_INTERNAL] != 0 && st == YB_OK) st = YB_ERR_INTERNAL;
+        if (errHost[EW_ERROR] || errHost[EW_WARNING] || errHost[EW_INTERNAL])
+            YB_CUDA(cudaMemsetAsync(d.err, 0, sizeof(int) * 3, S->stream));
+        return st;
+    }
+
+    int64_t penetrations() override { return penTotal; }
+
+    yb_status read_state_f64(double* pos, double* vel, double* q, double* dx, int buf) override {
+        const size_t n = (size_t)S->n;
+        double* tmp = nullptr;
+        YB_CUDA(cudaMalloc(&tmp, sizeof(double) * 14 * n));
+        double *dp = tmp, *dv = tmp + 3 * n, *dq = tmp + 6 * n, *ddx = tmp + 10 * n;
+        launch_state_f64(d, buf, pos ? dp : nullptr, vel ? dv : nullptr, q ? dq : nullptr, dx ? ddx : nullptr,
+                         S->stream);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess && pos) e = cudaMemcpyAsync(pos, dp, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, S->stream);
+        if (e == cudaSuccess && vel) e = cudaMemcpyAsync(vel, dv, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, S->stream);
+        if (e == cudaSuccess && q) e = cudaMemcpyAsync(q, dq, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, S->stream);
+        if (e == cudaSuccess && dx) e = cudaMemcpyAsync(dx, ddx, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, S->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(S->stream);
+        cudaFree(tmp);
+        return cuda_status(e);
+    }
+
+    yb_status contacts(int* numCols, int* cols, float* stepLimit) override {
+        const size_t n = (size_t)S->n;
+        cudaStream_t st = S->stream;
+        if (numCols) YB_CUDA(cudaMemcpyAsync(numCols, d.numCols, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+        if (cols) YB_CUDA(cudaMemcpyAsync(cols, d.cols, sizeof(int) * n * MAX_COLS, cudaMemcpyDeviceToHost, st));
+        if (stepLimit) {
+            if (sizeof(R) == 4) {
+                YB_CUDA(cudaMemcpyAsync(stepLimit, d.stepLim, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+            } else {
+                std::vector<R> tmp(n);
+                YB_CUDA(cudaMemcpyAsync(tmp.data(), d.stepLim, sizeof(R) * n, cudaMemcpyDeviceToHost, st));
+                YB_CUDA(cudaStreamSynchronize(st));
+                for (size_t i = 0; i < n; i++) stepLimit[i] = (float)tmp[i];
+            }
+        }
+        YB_CUDA(cudaStreamSynchronize(st));
+        return YB_OK;
+    }
+
+    yb_status bounds(int scene, float* out) override {
+        launch_scene_root_box(d, rootBoxes, S->stream);
+        S->launches++;
+        std::vector<float> b(6 * (size_t)S->numScenes);
+        YB_CUDA(cudaMemcpyAsync(b.data(), rootBoxes, sizeof(float) * b.size(), cudaMemcpyDeviceToHost, S->stream));
+        YB_CUDA(cudaStreamSynchronize(S->stream));
+        float r[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+        for (int s = 0; s < S->numScenes; s++) {
+            if (scene >= 0 && s != scene) continue;
+            for (int a = 0; a < 3; a++) {
+                r[a] = std::min(r[a], b[6 * s + a]);
+                r[3 + a] = std::max(r[3 + a], b[6 * s + 3 + a]);
+            }
+        }
+        std::memcpy(out, r, sizeof(r));
+        return YB_OK;
+    }
+
+    yb_status diagnostics(double* out) override {
+        write_params();
+        const int nb = launch_diag(d, diagPart, S->stream);
+        S->launches++;
+        std::vector<double> part(8 * (size_t)nb);
+        YB_CUDA(cudaGetLastError());
+        if (nb) YB_CUDA(cudaMemcpyAsync(part.data(), diagPart, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, S->stream));
+        YB_CUDA(cudaStreamSynchronize(S->stream));
+        double r[8] = {0, 0, 0, 0, 0, 0, INFINITY, 0};
+        for (int b = 0; b < nb; b++) {
+            for (int a = 0; a < 8; a++) {
+                const double v = part[8 * (size_t)b + a];
+                if (a == 5) r[a] = std::max(r[a], v);
+                else if (a == 6) r[a] = std::min(r[a], v);
+                else r[a] += v;
+            }
+        }
+        std::memcpy(out, r, sizeof(r));
+        return YB_OK;
+    }
+
+    uint64_t debug_phases(int mask, int& buf) override {
+        cudaStream_t st = S->stream;
+        uint64_t k = 0;
+        if (mask & 1) { launch_init(d, st); k++; buf = 0; }
+        if ((mask & 6) && d.nseg > 0) {
+            if (mask & 2) launch_bvh_rebuild(d, st, sortScratch, sortBytes, keyBits);
+            else launch_bvh_refit(d, st);
+            launch_traverse(d, st);
+            k += 2;
+        }
+        if (mask & 8) { launch_step_limit(d, st); k++; }
+        if (mask & 16) { launch_iter(d, buf, S->iterBlock, st); buf ^= 1; k++; }
+        if (mask & 32) { launch_end(d, buf, buf != 0, sizeof(R) == 4, st); buf = 0; k++; }
+        return k;
+    }
+};
+
+EngineBase* make_engine(yb_sim* S) {
+    if (S->precision == YB_PRECISION_FP64) return new (std::nothrow) Engine<double>(S);
+    return new (std::nothrow) Engine<float>(S);
+}
+
+yb_status engine_alloc(yb_sim* S) {
+    if (S->precision == YB_PRECISION_FP64) return static_cast<Engine<double>*>(S->eng)->alloc();
+    return static_cast<Engine<float>*>(S->eng)->alloc();
+}
+
+yb_status validate_all_meta(yb_sim* S) {
+    for (auto& m : S->meta) {
+        const yb_status st = upload_meta_checks(m);
+        if (st != YB_OK) return st;
+    }
+    return YB_OK;
+}
+
+}  // namespace
+
+// =========================================================================================
+extern "C" {
+
+yb_status yb_create_batch(int32_t numScenes, const int32_t* vertsPerScene, int32_t precision, yb_sim** out) {
+    if (!out || numScenes < 1 || !vertsPerScene) return YB_ERR_INVALID_ARGUMENT;
+    if (precision != YB_PRECISION_FP32 && precision != YB_PRECISION_FP64) return YB_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    long long total = 0;
+    for (int s = 0; s < numScenes; s++) {
+        if (vertsPerScene[s] < 3) return YB_ERR_TOO_FEW_VERTICES;
+        total += vertsPerScene[s];
+    }
+    if (total > (1LL << 31) / YB_MAX_COLLISIONS_PER_SEGMENT) return YB_ERR_INVALID_ARGUMENT;
+    yb_sim* S = new (std::nothrow) yb_sim();
+    if (!S) return YB_ERR_OUT_OF_MEMORY;
+    S->n = (int)total;
+    S->numScenes = numScenes;
+    S->precision = precision;
+    S->sceneOff.resize(numScenes + 1, 0);
+    for (int s = 0; s < numScenes; s++) S->sceneOff[s + 1] = S->sceneOff[s] + vertsPerScene[s];
+    S->meta.resize(numScenes);
+    for (int s = 0; s < numScenes; s++) default_meta(S->meta[s], vertsPerScene[s], S->maxH);
+    const size_t n = (size_t)total;
+    const size_t bytes = n * (sizeof(yb_vertex) + 12 + 16 + 16);
+    void* host = nullptr;
+    if (cudaHostAlloc(&host, bytes, cudaHostAllocDefault) == cudaSuccess) {
+        S->pinned = true;
+    } else {
+        cudaGetLastError();
+        host = std::malloc(bytes);
+        if (!host) { delete S; return YB_ERR_OUT_OF_MEMORY; }
+    }
+    S->verts = (yb_vertex*)host;
+    S->vels = (float*)((char*)host + sizeof(yb_vertex) * n);
+    S->qs = (float*)((char*)S->vels + 12 * n);
+    S->qRests = (float*)((char*)S->qs + 16 * n);
+    // Per-vertex defaults, YarnBall.cu:42-50
+    for (size_t i = 0; i < n; i++) {
+        yb_vertex& v = S->verts[i];
+        v.pos[0] = v.pos[1] = v.pos[2] = 0.f;
+        v.invMass = 1.f;
+        v.lRest = 1.f;
+        v.kStretch = 100.f;
+        v.connectionIndex = -1;
+        v.flags = YB_HAS_NEXT;
+        S->vels[3 * i] = S->vels[3 * i + 1] = S->vels[3 * i + 2] = 0.f;
+        S->qs[4 * i] = S->qs[4 * i + 1] = S->qs[4 * i + 2] = 0.f;
+        S->qs[4 * i + 3] = 1.f;
+        S->qRests[4 * i] = S->qRests[4 * i + 1] = S->qRests[4 * i + 2] = 0.f;
+        S->qRests[4 * i + 3] = 5.f;
+    }
+    for (int s = 0; s < numScenes; s++) S->verts[S->sceneOff[s + 1] - 1].flags = 0;
+    *out = S;
+    return YB_OK;
+}
+
+yb_status yb_create(int32_t numVerts, yb_sim** out) {
+    return yb_create_batch(1, &numVerts, YB_PRECISION_FP32, out);
+}
+
+void yb_destroy(yb_sim* S) {
+    if (!S) return;
+    if (S->stream) cudaStreamSynchronize(S->stream);
+    delete S->eng;
+    if (S->stream) cudaStreamDestroy(S->stream);
+    if (S->pinned)
+        cudaFreeHost(S->verts);
+    else
+        std::free(S->verts);
+    delete S;
+}
+
+yb_status yb_host_arrays(yb_sim* S, yb_vertex** verts, float** qs, float** qRests, float** vels) {
+    if (!S) return YB_ERR_INVALID_ARGUMENT;
+    if (verts) *verts = S->verts;
+    if (qs) *qs = S->qs;
+    if (qRests) *qRests = S->qRests;
+    if (vels) *vels = S->vels;
+    return YB_OK;
+}
+
+yb_status yb_get_meta(yb_sim* S, int32_t scene, yb_meta* out) {
+    if (!S || !out || scene < 0 || scene >= S->numScenes) return YB_ERR_INVALID_ARGUMENT;
+    *out = S->meta[scene];
+    return YB_OK;
+}
+
+yb_status yb_set_meta(yb_sim* S, int32_t scene, const yb_meta* in) {
+    if (!S || !in || scene < 0 || scene >= S->numScenes) return YB_ERR_INVALID_ARGUMENT;
+    const int n = S->meta[scene].numVerts;
+    S->meta[scene] = *in;
+    S->meta[scene].numVerts = n;  // fixed at creation
+    return YB_OK;
+}
+
+yb_status yb_get_max_h(yb_sim* S, float* maxH) {
+    if (!S || !maxH) return YB_ERR_INVALID_ARGUMENT;
+    *maxH = S->maxH;
+    return YB_OK;
+}
+
+yb_status yb_set_max_h(yb_sim* S, float maxH) {
+    if (!S || !(maxH > 0)) return YB_ERR_INVALID_ARGUMENT;
+    S->maxH = maxH;
+    return YB_OK;
+}
+
+yb_status yb_configure(yb_sim* S, float density) {
+    if (!S) return YB_ERR_INVALID_ARGUMENT;
+    S->initialInvMasses.assign(S->n, 0.f);
+    for (int s = 0; s < S->numScenes; s++) {
+        float mx = 0, mn = 0;
+        const yb_status st = configure_scene(S, S->sceneOff[s], S->sceneOff[s + 1] - S->sceneOff[s], density, mx, mn);
+        if (st != YB_OK) return st;
+        S->meta[s].maxSegLen = mx;
+        S->meta[s].minSegLen = mn;
+    }
+    if (S->eng) {  // re-configure: start from a fresh device state
+        if (S->stream) cudaStreamSynchronize(S->stream);
+        delete S->eng;
+        S->eng = nullptr;
+        S->configured = false;
+    }
+    if (!S->stream) {
+        cudaError_t e = cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            S->stream = nullptr;
+            return cuda_status(e);
+        }
+    }
+    S->eng = make_engine(S);
+    if (!S->eng) return YB_ERR_OUT_OF_MEMORY;
+    yb_status st = engine_alloc(S);
+    if (st != YB_OK) {
+        delete S->eng;
+        S->eng = nullptr;
+        return st;
+    }
+    S->configured = true;
+    st = validate_all_meta(S);
+    if (st != YB_OK) return st;
+    S->eng->write_params();
+    return S->eng->upload();
+}
+
+yb_status yb_set_kstretch(yb_sim* S, int32_t scene, float k) {
+    if (!S || scene >= S->numScenes) return YB_ERR_INVALID_ARGUMENT;
+    if (!S->configured) return YB_ERR_NOT_CONFIGURED;
+    const int s0 = scene < 0 ? 0 : scene, s1 = scene < 0 ? S->numScenes : scene + 1;
+    for (int i = S->sceneOff[s0]; i < S->sceneOff[s1]; i++) S->verts[i].kStretch = k * S->verts[i].lRest;
+    return YB_OK;
+}
+
+yb_status yb_set_kbend(yb_sim* S, int32_t scene, float k) {
+    if (!S || scene >= S->numScenes) return YB_ERR_INVALID_ARGUMENT;
+    if (!S->configured) return YB_ERR_NOT_CONFIGURED;
+    const int s0 = scene < 0 ? 0 : scene, s1 = scene < 0 ? S->numScenes : scene + 1;
+    k *= 4;
+    for (int i = S->sceneOff[s0]; i < S->sceneOff[s1]; i++) {
+        float* r = S->qRests + 4 * (size_t)i;
+        const float l = std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + r[3] * r[3]);
+        const float inv = 1.f / l;
+        const float s = k / S->verts[i].lRest;
+        const float a = r[0] * inv, b = r[1] * inv, c = r[2] * inv, w = r[3] * inv;
+        r[0] = s * a; r[1] = s * b; r[2] = s * c; r[3] = s * w;
+    }
+    return YB_OK;
+}
+
+yb_status yb_upload(yb_sim* S) {
+    if (!S) return YB_ERR_INVALID_ARGUMENT;
+    if (!S->configured) return YB_ERR_NOT_CONFIGURED;
+    return S->eng->upload();
+}
+
+yb_status yb_download(yb_sim* S) {
+    if (!S) return YB_ERR_INVALID_ARGUMENT;
+    if (!S->configured) return YB_ERR_NOT_CONFIGURED;
+    return S->eng->download();
+}
+
+yb_status yb_zero_velocities(yb_sim* S) {
+    if (!S) return YB_ERR_INVALID_ARGUMENT;
+    if (!S->configured) return YB_ERR_NOT_CONFIGURED;
+    return S->eng->zero_vel();
+}
+
+yb_status yb_advance(yb_sim* S, float dt, float* advanced) {
+    if (!S) return YB_ERR_INVALID_ARGUMENT;
+    if (advanced) *advanced = 0.f;
+    if (!S->configured) return YB_ERR_NOT_CONFIGURED;
+    if (!(dt > 0)) return YB_OK;
+    // step.cpp:101-120
+    const int steps = std::max(1, (int)std::ceil(dt / S->maxH));
+    for (auto& m : S->meta) {
+        m.lastH = m.h;
+        m.h = dt / steps;
+    }
+    yb_status st = validate_all_meta(S);
+    if (st != YB_OK) return st;
+    S->eng->write_params();
+    const yb_meta& m0 = S->meta[0];
+    for (int s = 0; s < steps; s++, S->stepCounter++) {
+        int type = 2;
+        if (m0.detectionPeriod > 0 && S->stepCounter % (uint64_t)m0.detectionPeriod == 0) {
+            // collision.cu:101-108
+            if (S->lastBVHRebuild >= m0.bvhRebuildPeriod) {
+                type = 0;
+                S->lastBVHRebuild = 0;
+            } else {
+                type = 1;
+                S->lastBVHRebuild += m0.h * m0.detectionPeriod;
+            }
+        }
+        st = S->eng->run_substep(type);
+        if (st != YB_OK) return st;
+    }
+    for (auto& m : S->meta) m.time += dt;
+    st = S->eng->check_errors();
+    if (advanced) *advanced = dt;
+    return st;
+}
+
+yb_status yb_step(yb_sim* S, float) {
+    if (!S) return YB_ERR_INVALID_ARGUMENT;
+    return yb_advance(S, S->maxH, nullptr);
+}
+
+yb_status yb_step_count(yb_sim* S, uint64_t* out) {
+    if (!S || !out) return YB_ERR_INVALID_ARGUMENT;
+    *out = S->stepCounter;
+    return YB_OK;
+}
+
+yb_status yb_bounds(yb_sim* S, int32_t scene, float minmax[6]) {
+    if (!S || !minmax || scene >= S->numScenes) return YB_ERR_INVALID_ARGUMENT;
+    if (!S->configured) return YB_ERR_NOT_CONFIGURED;
+    return S->eng->bounds(scene, minmax);
+}
+
+yb_status yb_collision_stats(yb_sim* S, uint64_t* totalPairs, int32_t* segmentsWithContacts, int32_t* maxPerSegment) {
+    if (!S) return YB_ERR_INVALID_ARGUMENT;
+    if (!S->configured) return YB_ERR_NOT_CONFIGURED;
+    std::vector<int> nc(S->n);
+    const yb_status st = S->eng->contacts(nc.data(), nullptr, nullptr);
+    if (st != YB_OK) return st;
+    uint64_t tot = 0;
+    int segs = 0, mx = 0;
+    for (int c : nc) {
+        if (c > 0) { tot += c; segs++; }
+        mx = std::max(mx, c);
+    }
+    if (totalPairs) *totalPairs = tot / 2;
+    if (segmentsWithContacts) *segmentsWithContacts = segs;
+    if (maxPerSegment) *maxPerSegment = mx;
+    return YB_OK;
+}
+
+yb_status yb_last_error(yb_sim* S, int32_t* errorCode, int32_t* warningCode) {
+    if (!S) return YB_ERR_INVALID_ARGUMENT;
+    if (errorCode) *errorCode = S->lastErrorCode;
+    if (warningCode) *warningCode = S->lastWarningCode;
+    return YB_OK;
+}
+
+yb_status yb_initial_inv_masses(yb_sim* S, const float** out, int32_t* count) {
+    if (!S || !out) return YB_ERR_INVALID_ARGUMENT;
+    *out = S->initialInvMasses.empty() ? nullptr : S->initialInvMasses.data();
+    if (count) *count = (int32_t)S->initialInvMasses.size();
+    return YB_OK;
+}
+
+const char* yb_status_string(yb_status s) {
+    switch (s) {
+        case YB_OK: return "ok";
+        case YB_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case YB_ERR_TOO_FEW_VERTICES: return "Too little vertices";
+        case YB_ERR_NOT_CONFIGURED: return "No rest length. Must call configure()";
+        case YB_ERR_DANGLING_SEGMENT: return "Dangling segment. Yarns must be atleast 2 segments long";
+        case YB_ERR_ZERO_LENGTH_SEGMENT: return "0 length segment";
+        case YB_ERR_DETECTION_SCALER: return "Detection scaler must be greater than 1.";
+        case YB_ERR_SEGMENT_TOO_SHORT:
+            return "Use thinner yarn or use longer segments. (2 * Min seg length must be at least 2 * radius + barrierThickness";
+        case YB_ERR_MAX_COLLISIONS_PER_SEGMENT_EXCEEDED: return "MAX_COLLISIONS_PER_SEGMENT exceeded";
+        case YB_ERR_CUDA: return "CUDA error";
+        case YB_ERR_OUT_OF_MEMORY: return "out of device or host memory";
+        case YB_ERR_INTERNAL: return "internal error: a bounded device wait expired or the BVH stack overflowed";
+        case YB_ERR_ALREADY_CONFIGURED: return "already configured";
+    }
+    return "unknown status";
+}
+
+yb_status yb_set_tuning(yb_sim* S, int32_t iterBlock, int32_t useGraphs) {
+    if (!S) return YB_ERR_INVALID_ARGUMENT;
+    if (iterBlock != 64 && iterBlock != 128 && iterBlock != 256 && iterBlock != 512) return YB_ERR_INVALID_ARGUMENT;
+    S->iterBlock = iterBlock;
+    S->useGraphs = useGraphs ? 1 : 0;
+    if (S->eng) S->eng->invalidate_graphs();
+    return YB_OK;
+}
+
+yb_status yb_get_tuning(yb_sim* S, int32_t* iterBlock, int32_t* useGraphs) {
+    if (!S) return YB_ERR_INVALID_ARGUMENT;
+    if (iterBlock) *iterBlock = S->iterBlock;
+    if (useGraphs) *useGraphs = S->useGraphs;
+    return YB_OK;
+}
+
+yb_status yb_launch_count(yb_sim* S, uint64_t* out) {
+    if (!S || !out) return YB_ERR_INVALID_ARGUMENT;
+    *out = S->launches;
+    return YB_OK;
+}
+
+yb_status yb_info(yb_sim* S, int32_t* numVerts, int32_t* numScenes, int32_t* precision) {
+    if (!S) return YB_ERR_INVALID_ARGUMENT;
+    if (numVerts) *numVerts = S->n;
+    if (numScenes) *numScenes = S->numScenes;
+    if (precision) *precision = S->precision;
+    return YB_OK;
+}
+
+yb_status yb_penetration_count(yb_sim* S, int64_t* out) {
+    if (!S || !out) return YB_ERR_INVALID_ARGUMENT;
+    if (!S->configured) return YB_ERR_NOT_CONFIGURED;
+    const yb_status st = S->eng->check_errors();
+    *out = S->eng->penetrations();
+    return st == YB_ERR_MAX_COLLISIONS_PER_SEGMENT_EXCEEDED ? YB_OK : st;
+}
+
+yb_status yb_diagnostics(yb_sim* S, double out[8]) {
+    if (!S || !out) return YB_ERR_INVALID_ARGUMENT;
+    if (!S->configured) return YB_ERR_NOT_CONFIGURED;
+    return S->eng->diagnostics(out);
+}
+
+yb_status yb_read_state_f64(yb_sim* S, double* pos, double* vel, double* q) {
+    if (!S) return YB_ERR_INVALID_ARGUMENT;
+    if (!S->configured) return YB_ERR_NOT_CONFIGURED;
+    return S->eng->read_state_f64(pos, vel, q, nullptr, 0);
+}
+
+yb_status yb_debug_contacts(yb_sim* S, int32_t* numCols, int32_t* cols, float* stepLimit) {
+    if (!S) return YB_ERR_INVALID_ARGUMENT;
+    if (!S->configured) return YB_ERR_NOT_CONFIGURED;
+    return S->eng->contacts(numCols, cols, stepLimit);
+}
+
+yb_status yb_debug_dx(yb_sim* S, double* dx4) {
+    if (!S || !dx4) return YB_ERR_INVALID_ARGUMENT;
+    if (!S->configured) return YB_ERR_NOT_CONFIGURED;
+    return S->eng->read_state_f64(nullptr, nullptr, nullptr, dx4, S->dbgBuf);
+}
+
+yb_status yb_debug_phases(yb_sim* S, int32_t mask, float h) {
+    if (!S) return YB_ERR_INVALID_ARGUMENT;
+    if (!S->configured) return YB_ERR_NOT_CONFIGURED;
+    if (h > 0) {
+        for (auto& m : S->meta) {
+            m.lastH = m.h;
+            m.h = h;
+        }
+    }
+    yb_status st = validate_all_meta(S);
+    if (st != YB_OK) return st;
+    S->eng->write_params();
+    S->launches += S->eng->debug_phases(mask, S->dbgBuf);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_status(e);
+    return S->eng->check_errors();
+}
+
+yb_status yb_debug_sort_pairs(const uint64_t* keys, const int32_t* vals, int32_t n, int32_t bits, uint64_t* keysOut,
+                              int32_t* valsOut) {
+    if (n < 0 || (n > 0 && (!keys || !vals || !keysOut || !valsOut)) || bits < 0 || bits > 64)
+        return YB_ERR_INVALID_ARGUMENT;
+    if (n == 0) return YB_OK;
+    const size_t scratch = radix_sort_scratch_bytes(n);
+    char* mem = nullptr;
+    const size_t kb = sizeof(unsigned long long) * (size_t)n, vb = sizeof(int) * (size_t)n;
+    YB_CUDA(cudaMalloc(&mem, 2 * kb + 2 * vb + scratch + 256));
+    unsigned long long* k[2] = {(unsigned long long*)mem, (unsigned long long*)(mem + kb)};
+    int* v[2] = {(int*)(mem + 2 * kb), (int*)(mem + 2 * kb + vb)};
+    void* scr = mem + 2 * kb + 2 * vb;
+    int* err = (int*)((char*)scr + scratch);
+    cudaError_t e = cudaMemcpy(k[0], keys, kb, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(v[0], vals, vb, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(err, 0, sizeof(int));
+    int buf = 0;
+    if (e == cudaSuccess) {
+        buf = radix_sort_pairs(k, v, n, bits, scr, err, 0);
+        e = cudaGetLastError();
+    }
+    int herr = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(keysOut, k[buf], kb, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(valsOut, v[buf], vb, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(&herr, err, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(mem);
+    if (e != cudaSuccess) return cuda_status(e);
+    return herr ? YB_ERR_INTERNAL : YB_OK;
+}
+
+}  // extern "C"

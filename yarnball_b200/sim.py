@@ -1,0 +1,264 @@
+"""Python mirror of YarnBall::Sim (KittenEngine/YarnBall/YarnBall.h:116-206).
+
+Same names, argument meaning and error behaviour as the C++ class: the host arrays
+`verts`, `qs`, `qRests`, `vels` are numpy views of the library-owned host memory, `meta`
+reads and writes the MetaData fields, and failures raise RuntimeError (YarnBallError)
+where the reference throws std::runtime_error.  All computation happens in the CUDA engine
+behind the C ABI.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _abi
+from ._abi import YbMeta, check, ptr
+
+
+class VertexFlags:
+    """YarnBall::VertexFlags, YarnBall.h:34-40."""
+
+    hasPrev = 1
+    hasNext = 2
+    hasNextOrientation = 4
+    fixOrientation = 8
+    colliding = 16
+
+
+MAX_COLLISIONS_PER_SEGMENT = 128
+
+
+class _MetaView:
+    """Attribute access to one scene's MetaData; every write goes through yb_set_meta."""
+
+    def __init__(self, sim, scene):
+        object.__setattr__(self, "_sim", sim)
+        object.__setattr__(self, "_scene", scene)
+
+    def _get(self):
+        m = YbMeta()
+        check(self._sim._lib.yb_get_meta(self._sim._h, self._scene, ctypes.byref(m)), "meta")
+        return m
+
+    def __getattr__(self, name):
+        v = getattr(self._get(), name)
+        if isinstance(v, ctypes.Array):
+            return np.array(v[:], dtype=np.float32)
+        return v
+
+    def __setattr__(self, name, value):
+        m = self._get()
+        cur = getattr(m, name)
+        if isinstance(cur, ctypes.Array):
+            for i, x in enumerate(value):
+                cur[i] = x
+        else:
+            setattr(m, name, value)
+        check(self._sim._lib.yb_set_meta(self._sim._h, self._scene, ctypes.byref(m)), "meta")
+
+    def as_struct(self):
+        return self._get()
+
+
+class Sim:
+    ERROR_NONE = 0
+    ERROR_MAX_COLLISIONS_PER_SEGMENT_EXCEEDED = 1
+    WARNING_SEGMENT_INTERPENETRATION = 2
+
+    def __init__(self, numVerts=None, *, scenes=None, precision="fp32"):
+        """Sim(numVerts) as YarnBall.cu:11-51, or a batch of independent scenes
+        (scenes = list of vertex counts).  precision: "fp32" or "fp64"."""
+        self._lib = _abi.load()
+        self._h = ctypes.c_void_p()
+        prec = {"fp32": 0, "fp64": 1}[precision]
+        if scenes is None:
+            if numVerts is None:
+                raise ValueError("numVerts or scenes required")
+            scenes = [int(numVerts)]
+        counts = np.ascontiguousarray(np.asarray(scenes, dtype=np.int32))
+        check(self._lib.yb_create_batch(len(counts), ptr(counts, ctypes.c_int32), prec, ctypes.byref(self._h)), "Sim")
+        self.numScenes = len(counts)
+        self.sceneOffsets = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+        self.numVerts = int(self.sceneOffsets[-1])
+        self.precision = precision
+        vp = ctypes.c_void_p()
+        qp, qrp, vlp = _abi.c_float_p(), _abi.c_float_p(), _abi.c_float_p()
+        check(self._lib.yb_host_arrays(self._h, ctypes.byref(vp), ctypes.byref(qp), ctypes.byref(qrp),
+                                       ctypes.byref(vlp)), "host arrays")
+        n = self.numVerts
+        raw = (ctypes.c_char * (32 * n)).from_address(vp.value)
+        self.verts = np.frombuffer(raw, dtype=_abi.VERTEX_DTYPE, count=n)
+        self.qs = np.ctypeslib.as_array(qp, shape=(n, 4))
+        self.qRests = np.ctypeslib.as_array(qrp, shape=(n, 4))
+        self.vels = np.ctypeslib.as_array(vlp, shape=(n, 3))
+        self.meta = _MetaView(self, 0)
+        self.printErrors = True
+
+    # ---- lifecycle -------------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.yb_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- parameters ------------------------------------------------------------------
+    def scene_meta(self, scene):
+        return _MetaView(self, scene)
+
+    def set_meta_all(self, **fields):
+        """Sets the same MetaData fields on every scene of a batch."""
+        for s in range(self.numScenes):
+            mv = self.scene_meta(s)
+            for k, v in fields.items():
+                setattr(mv, k, v)
+
+    @property
+    def maxH(self):
+        v = ctypes.c_float()
+        check(self._lib.yb_get_max_h(self._h, ctypes.byref(v)))
+        return v.value
+
+    @maxH.setter
+    def maxH(self, value):
+        check(self._lib.yb_set_max_h(self._h, float(value)), "maxH")
+
+    # ---- YarnBall::Sim API -----------------------------------------------------------
+    def configure(self, density=1e-3):
+        check(self._lib.yb_configure(self._h, float(density)), "configure")
+
+    def setKBend(self, k=3e-9, scene=-1):
+        check(self._lib.yb_set_kbend(self._h, int(scene), float(k)), "setKBend")
+
+    def setKStretch(self, k=1e-2, scene=-1):
+        check(self._lib.yb_set_kstretch(self._h, int(scene), float(k)), "setKStretch")
+
+    def upload(self):
+        check(self._lib.yb_upload(self._h), "upload")
+
+    def download(self):
+        check(self._lib.yb_download(self._h), "download")
+
+    def zeroVelocities(self):
+        check(self._lib.yb_zero_velocities(self._h), "zeroVelocities")
+
+    def advance(self, dt):
+        out = ctypes.c_float()
+        st = self._lib.yb_advance(self._h, float(dt), ctypes.byref(out))
+        if st != 0 and self.printErrors:
+            import sys
+
+            sys.stderr.write("ERROR: %s\n" % self._lib.yb_status_string(st).decode())
+        check(st, "advance")
+        return out.value
+
+    def step(self, dt=None):
+        check(self._lib.yb_step(self._h, float(dt or 0.0)), "step")
+
+    def stepCount(self):
+        v = ctypes.c_uint64()
+        check(self._lib.yb_step_count(self._h, ctypes.byref(v)))
+        return v.value
+
+    def bounds(self, scene=-1):
+        b = np.zeros(6, dtype=np.float32)
+        check(self._lib.yb_bounds(self._h, int(scene), ptr(b, ctypes.c_float)), "bounds")
+        return b[:3].copy(), b[3:].copy()
+
+    def collisionStats(self):
+        tot, segs, mx = ctypes.c_uint64(), ctypes.c_int32(), ctypes.c_int32()
+        check(self._lib.yb_collision_stats(self._h, ctypes.byref(tot), ctypes.byref(segs), ctypes.byref(mx)))
+        return int(tot.value), int(segs.value), int(mx.value)
+
+    def printCollisionStats(self):
+        tot, segs, _ = self.collisionStats()
+        print("Total collisions: %d" % tot)
+        print("Segments with collisions: %d/%d" % (segs, self.numVerts))
+
+    @property
+    def lastErrorCode(self):
+        e, w = ctypes.c_int32(), ctypes.c_int32()
+        check(self._lib.yb_last_error(self._h, ctypes.byref(e), ctypes.byref(w)))
+        return e.value
+
+    @property
+    def lastWarningCode(self):
+        e, w = ctypes.c_int32(), ctypes.c_int32()
+        check(self._lib.yb_last_error(self._h, ctypes.byref(e), ctypes.byref(w)))
+        return w.value
+
+    @property
+    def initialInvMasses(self):
+        p = _abi.c_float_p()
+        c = ctypes.c_int32()
+        check(self._lib.yb_initial_inv_masses(self._h, ctypes.byref(p), ctypes.byref(c)))
+        if c.value == 0:
+            return np.zeros(0, np.float32)
+        return np.ctypeslib.as_array(p, shape=(c.value,)).copy()
+
+    # ---- additions -------------------------------------------------------------------
+    def set_tuning(self, iterBlock=256, useGraphs=True):
+        check(self._lib.yb_set_tuning(self._h, int(iterBlock), 1 if useGraphs else 0), "tuning")
+
+    def launch_count(self):
+        v = ctypes.c_uint64()
+        check(self._lib.yb_launch_count(self._h, ctypes.byref(v)))
+        return int(v.value)
+
+    def penetrations(self):
+        v = ctypes.c_int64()
+        check(self._lib.yb_penetration_count(self._h, ctypes.byref(v)))
+        return int(v.value)
+
+    def diagnostics(self):
+        """FP64 energies and contact statistics of the device state (see yarnball_b200.h)."""
+        out = np.zeros(8, np.float64)
+        check(self._lib.yb_diagnostics(self._h, ptr(out, ctypes.c_double)), "diagnostics")
+        keys = ["kinetic", "gravity", "stretch", "bend", "barrier", "max_speed", "min_gap", "pairs"]
+        return dict(zip(keys, out.tolist()))
+
+    def read_state_f64(self):
+        n = self.numVerts
+        pos = np.zeros((n, 3)); vel = np.zeros((n, 3)); q = np.zeros((n, 4))
+        check(self._lib.yb_read_state_f64(self._h, ptr(pos, ctypes.c_double), ptr(vel, ctypes.c_double),
+                                          ptr(q, ctypes.c_double)), "read_state")
+        return pos, vel, q
+
+    def debug_contacts(self):
+        n = self.numVerts
+        nc = np.zeros(n, np.int32)
+        cols = np.zeros(n * MAX_COLLISIONS_PER_SEGMENT, np.int32)
+        sl = np.zeros(n, np.float32)
+        check(self._lib.yb_debug_contacts(self._h, ptr(nc, ctypes.c_int32), ptr(cols, ctypes.c_int32),
+                                          ptr(sl, ctypes.c_float)), "contacts")
+        lists = [np.sort(cols[i + n * np.arange(nc[i])]) if nc[i] else np.zeros(0, np.int32) for i in range(n)]
+        return nc, lists, sl
+
+    def debug_dx(self):
+        dx = np.zeros((self.numVerts, 4))
+        check(self._lib.yb_debug_dx(self._h, ptr(dx, ctypes.c_double)), "dx")
+        return dx[:, :3].copy()
+
+    def debug_phases(self, mask, h=0.0):
+        check(self._lib.yb_debug_phases(self._h, int(mask), float(h)), "phases")
+
+
+def sort_pairs(keys, vals, bits):
+    """Device radix sort of (uint64 key, int32 value) pairs by the low `bits` bits."""
+    lib = _abi.load()
+    k = np.ascontiguousarray(keys, dtype=np.uint64)
+    v = np.ascontiguousarray(vals, dtype=np.int32)
+    ko = np.zeros_like(k)
+    vo = np.zeros_like(v)
+    check(lib.yb_debug_sort_pairs(ptr(k, ctypes.c_uint64), ptr(v, ctypes.c_int32), len(k), int(bits),
+                                  ptr(ko, ctypes.c_uint64), ptr(vo, ctypes.c_int32)), "sort")
+    return ko, vo
