@@ -1,0 +1,414 @@
+#!/usr/bin/env python
+"""Benchmark: vertex-substeps/s of the batched Stable Cosserat Rods substep on B200.
+
+Workload (one "step" = one advance(1/30 s) of every scene = 34 substeps x 8 Newton
+iterations): the batched uneven-scene configuration - up to 512 independent random-walk
+yarn piles (k ~ U{1..64} yarns, 64..4096 vertices per yarn, log-uniform), added until the
+next scene would pass 8,388,608 vertices; per-scene kBend log-uniform in [1e-9, 1e-7],
+kStretch 2e-2, kCollision 1e-7, mu 0.3, yarn radius 0.5 mm, gravity -9.8, first vertex of
+each yarn pinned.  Synthetic, seeded (no dataset exists for this path).
+
+  python bench.py [--gpus N --steps K --warmup W]      # the CUDA engine (one JSON line)
+  python bench.py --impl reference ...                 # the reference algorithm on the host
+
+Under torchrun every rank simulates its own batch (seed offset by rank): weak scaling, no
+collective on the data path; the time is the max over ranks of the device time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "vertex-substeps/s on 1 B200, batched vs plain at ≤1e-4 rel err vs FP64; HBM %"
+UNIT = "vertex-substeps/s"
+FRAME = 1.0 / 30.0
+MAX_H = 1e-3
+SUBSTEPS = int(np.ceil(np.float32(FRAME) / np.float32(MAX_H)))  # 34
+NUM_ITR = 8
+SEED = 7
+# Algorithmic bytes per vertex per Newton iteration (position solve 92 + orientation 84)
+# plus 4 bytes per contact-list entry: the per-unit figure of the roofline.
+ITER_BYTES_BASE = 176
+ITER_BYTES_PER_CONTACT = 4
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--no-plain", action="store_true", help="skip the plain per-scene advance() loop")
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    p.add_argument("--cap", type=int, default=8388608, help="vertex cap of the batched workload")
+    return p.parse_args()
+
+
+def workload_desc(spec):
+    yarns, lens, _ = spec
+    n = int(sum(int(l.sum()) for l in lens))
+    return n, {
+        "workload": "batched uneven scenes: %d random-walk yarn piles, %d vertices, %d yarns" % (
+            len(yarns), n, int(sum(yarns))),
+        "scenes": len(yarns),
+        "vertices": n,
+        "substeps_per_step": SUBSTEPS,
+        "newton_iterations": NUM_ITR,
+        "step": "advance(1/30 s) of the whole batch (%d substeps of h=1/%d s)" % (SUBSTEPS, SUBSTEPS * 30),
+        "l2": "inputs larger than L2 (state ~0.8 KB/vertex x %.1fM vertices), no flush" % (n / 1e6),
+        "seed": SEED,
+        "parallelism": "one independent batch per GPU (weak scaling)",
+    }
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.gpu_id = gpu_id
+        self.lines = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu_id), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.th.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def load_traffic():
+    """Per-vertex DRAM bytes of one Newton iteration from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "k_iter_traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+def oracle_sample(spec, target_verts, mode, seed=SEED):
+    """The first scenes of the batch totalling >= target_verts vertices, assembled and
+    configured on the oracle side (same geometry and parameters as the GPU batch)."""
+    import oracle
+    from yarnball_b200 import scenes
+
+    yarns, lens, kbend = spec
+    k, tot = 0, 0
+    while k < len(yarns) and tot < target_verts:
+        tot += int(lens[k].sum())
+        k += 1
+    flat = np.concatenate(lens).astype(np.int32)
+    pos_all = scenes.random_walks_batch(seed, yarns, flat)
+    counts = [int(l.sum()) for l in lens[:k]]
+    offs = np.concatenate([[0], np.cumsum(counts)])
+    pos_list = [pos_all[offs[s]:offs[s + 1]] for s in range(k)]
+    orc = oracle.build_scenes(pos_list, lens[:k], kbend[:k], scenes.PILE_META, mode=mode)
+    return orc, k, tot
+
+
+def cpu_baseline_sample(spec, target_verts=1_000_000, reps_seconds=10.0, mode=None):
+    """The oracle (FP32 as the reference writes it, OpenMP over all host cores) on the first
+    scenes of the batch totalling >= target_verts vertices: one substep per repetition."""
+    import oracle
+    from yarnball_b200 import scenes
+
+    orc, k, tot = oracle_sample(spec, target_verts, oracle.FP32 if mode is None else mode)
+    h = float(np.float32(FRAME) / np.float32(SUBSTEPS))
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        orc.advance(h, h)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= reps_seconds or reps >= 50:
+            break
+    return {"value": tot * reps / el, "unit": UNIT, "cores": oracle.max_threads(), "kind": "port",
+            "sample": "first %d scenes (%d vertices) of the same batch, %d substep(s) of h=1/%d s, FP32 OpenMP"
+                      % (k, tot, reps, SUBSTEPS * 30), "seconds": el}
+
+
+def run_reference(args):
+    """Reference arm: the reference's algorithm as restated by the CPU oracle (the reference
+    itself does not build here), FP32, all host threads; each step = one substep of a bounded
+    sample of the batch."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle
+    from yarnball_b200 import scenes
+
+    spec = scenes.batched_spec(SEED, 512, args.cap)
+    n, cfg = workload_desc(spec)
+    orc, k, tot = oracle_sample(spec, 400_000, oracle.FP32)
+    h = float(np.float32(FRAME) / np.float32(SUBSTEPS))
+    for _ in range(args.warmup):
+        orc.advance(h, h)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        orc.advance(h, h)
+    el = time.perf_counter() - t0
+    value = tot * args.steps / el
+    cores = oracle.max_threads()
+    sample = "first %d scenes (%d vertices) of the batch, one substep of h=1/%d s per step" % (k, tot, SUBSTEPS * 30)
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": cfg,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference (CUDA/MSBuild, needs glm, jsoncpp and an absent LBVH submodule) does not build "
+                "offline; its substep is run as the CPU restatement in oracle/ (strict Jacobi, FP32, OpenMP)",
+    }
+    print(json.dumps(out))
+
+
+def run_ours(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from yarnball_b200 import scenes
+
+    spec = scenes.batched_spec(SEED + 1000 * rank, 512, args.cap)
+    n, cfg = workload_desc(spec)
+    sim, _ = scenes.build_batched(seed=SEED + 1000 * rank, spec=spec)
+    stream = torch.cuda.Stream()
+    sim.set_stream(stream.cuda_stream)
+    for _ in range(args.warmup):
+        sim.advance(FRAME)
+    try:
+        uuid = str(torch.cuda.get_device_properties(local).uuid)
+        gpu_id = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+    except Exception:
+        gpu_id = os.environ.get("CUDA_VISIBLE_DEVICES", str(local)).split(",")[local]
+    clocks = ClockSampler(gpu_id)
+    clocks.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = sim.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        sim.advance(FRAME)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ck = clocks.stop()
+    launches = sim.launch_count() - l0
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms, float(n)], device="cuda", dtype=torch.float64)
+    if dist:
+        tmax = t.clone()
+        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
+        tsum = t.clone()
+        dist.all_reduce(tsum[1:], op=dist.ReduceOp.SUM)
+        ms_max, n_all = float(tmax[0]), float(tsum[1])
+    else:
+        ms_max, n_all = ms, float(n)
+    value = n_all * SUBSTEPS * args.steps / (ms_max / 1e3)
+
+    # Per-kernel device times of one more frame (events around each kernel class).
+    prof_ms, prof_launches = sim.profile_advance(FRAME)
+    total_pairs, segs_with, max_cols = sim.collisionStats()
+    nseg = int(((sim.verts["flags"] & 2) != 0).sum())
+    cbar = 2.0 * total_pairs / max(nseg, 1)
+    iter_launches = max(1, prof_launches["iter"])
+    iter_ms = prof_ms["iter"] / iter_launches
+    bytes_per_launch = n * (ITER_BYTES_BASE + ITER_BYTES_PER_CONTACT * cbar)
+    achieved = bytes_per_launch / (iter_ms / 1e3) / 1e9
+    peak, peak_kind = load_peaks()
+    tr = load_traffic()
+    traffic = None
+    if tr:
+        traffic = tr["dram_bytes_per_vertex"] * n
+    prof_total = sum(prof_ms.values())
+    roofline = {
+        "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+        "traffic": traffic, "kernel": "k_iter (fused Newton position solve + orientation update)",
+        "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+        "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": iter_ms, "cbar": cbar,
+        "kernel_share": {k: v / prof_total for k, v in prof_ms.items()},
+        "kernel_ms_per_frame": prof_ms,
+    }
+
+    # End to end through the public API with host buffers: upload + advance + download.
+    h2d = n * (32 + 12 + 16 + 16)
+    d2h = n * (32 + 12 + 16)
+    sim.download()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    w0 = time.perf_counter()
+    f0.record(stream)
+    e2e_steps = max(2, args.steps // 2)
+    for _ in range(e2e_steps):
+        sim.upload()
+        sim.advance(FRAME)
+        sim.download()
+    f1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - w0
+    ems = f0.elapsed_time(f1)
+    if dist:
+        tt = torch.tensor([ems], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ems = float(tt[0])
+    e2e = {"value": n_all * SUBSTEPS * e2e_steps / (ems / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": d2h, "steps": e2e_steps, "wall_s": wall,
+           "api": "yb_upload + yb_advance + yb_download (pinned host arrays)"}
+
+    diag = sim.diagnostics()
+    pens = sim.penetrations()
+    plain = None
+    if not args.no_plain and rank == 0 and world == 1:
+        plain = run_plain(spec, stream)
+    sim.close()
+    cpu = None
+    if not args.no_cpu and rank == 0 and world == 1:
+        cpu = cpu_baseline_sample(spec)
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches) * world,
+            "clocks": ck, "plain": plain,
+            "batched_over_plain": (value / plain["value"]) if plain else None,
+            "contacts": {"pairs": total_pairs, "segments_with_contacts": segs_with, "max_per_segment": max_cols,
+                         "cbar": cbar},
+            "interpenetrations": pens, "diagnostics": diag,
+        }
+        print(json.dumps(out))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_plain(spec, stream):
+    """The drop-in path: one Sim per scene, advance() called scene after scene."""
+    import torch
+
+    from yarnball_b200 import scenes
+
+    yarns, lens, kbend = spec
+    flat = np.concatenate(lens).astype(np.int32)
+    pos_all = scenes.random_walks_batch(SEED, yarns, flat)
+    counts = [int(l.sum()) for l in lens]
+    sims = []
+    off = 0
+    for s in range(len(yarns)):
+        sm = scenes.Sim(counts[s])
+        scenes.fill_yarns(sm, pos_all[off:off + counts[s]], lens[s], pin_first=True)
+        for k, val in scenes.PILE_META.items():
+            setattr(sm.meta, k, val)
+        sm.configure()
+        sm.setKBend(kbend[s])
+        sm.setKStretch(2e-2)
+        sm.maxH = MAX_H
+        sm.upload()
+        sm.set_stream(stream.cuda_stream)
+        sims.append(sm)
+        off += counts[s]
+    for sm in sims:
+        sm.advance(FRAME)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    steps = 2
+    l0 = sum(sm.launch_count() for sm in sims)
+    e0.record(stream)
+    for _ in range(steps):
+        for sm in sims:
+            sm.advance(FRAME)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = sum(sm.launch_count() for sm in sims) - l0
+    for sm in sims:
+        sm.close()
+    n = sum(counts)
+    return {"value": n * SUBSTEPS * steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps, "steps": steps,
+            "gpu_launches": int(launches), "scenes": len(sims)}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

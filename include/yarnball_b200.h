@@ -178,6 +178,18 @@ const char* yb_status_string(yb_status s);
 yb_status yb_set_tuning(yb_sim* sim, int32_t iterBlock, int32_t useGraphs);
 yb_status yb_get_tuning(yb_sim* sim, int32_t* iterBlock, int32_t* useGraphs);
 
+/* Launch the simulation's work on `stream` (a cudaStream_t; NULL returns to the simulation's
+ * own stream).  Lets a caller order the engine with its own work and time it with events. */
+yb_status yb_set_stream(yb_sim* sim, void* stream);
+
+/* advance(dt) with every kernel class bracketed by CUDA events on the simulation's stream
+ * (no graphs): msByClass[c] accumulates device milliseconds and launchesByClass[c] the
+ * launches of class c: 0 predictor, 1 BVH rebuild (bounds, Morton, sort, Karras, refit),
+ * 2 BVH refit, 3 traversal + step limit, 4 step limit alone, 5 Newton/orientation
+ * iteration, 6 advection.  Arrays hold YB_PROFILE_CLASSES entries. */
+#define YB_PROFILE_CLASSES 7
+yb_status yb_profile_advance(yb_sim* sim, float dt, double* msByClass, uint64_t* launchesByClass);
+
 /* Kernels launched on the device so far (each graph node counts once per replay). */
 yb_status yb_launch_count(yb_sim* sim, uint64_t* out);
 

@@ -171,6 +171,96 @@ class OracleSim:
         return int(self.lib.orc_penetrations(self.h))
 
 
+class OrcMeta(ctypes.Structure):
+    """orc_meta (same layout as the reference MetaData host fields)."""
+
+    _fields_ = [
+        ("gravity", ctypes.c_float * 3), ("numItr", ctypes.c_int32), ("worldFloorNormal", ctypes.c_float * 3),
+        ("worldFloorPos", ctypes.c_float), ("h", ctypes.c_float), ("lastH", ctypes.c_float), ("time", ctypes.c_float),
+        ("numVerts", ctypes.c_int32), ("damping", ctypes.c_float), ("drag", ctypes.c_float),
+        ("frictionCoeff", ctypes.c_float), ("kCollision", ctypes.c_float), ("kFriction", ctypes.c_float),
+        ("detectionRadius", ctypes.c_float), ("scaledDetectionRadius", ctypes.c_float), ("radius", ctypes.c_float),
+        ("accelerationRatio", ctypes.c_float), ("barrierThickness", ctypes.c_float),
+        ("detectionScaler", ctypes.c_float), ("bvhRebuildPeriod", ctypes.c_float), ("detectionPeriod", ctypes.c_int32),
+        ("maxSegLen", ctypes.c_float), ("minSegLen", ctypes.c_float), ("useStepSizeLimit", ctypes.c_int32),
+        ("useVelocityRadius", ctypes.c_int32),
+    ]
+
+
+VERTEX_DTYPE = np.dtype([("pos", "<f4", (3,)), ("invMass", "<f4"), ("lRest", "<f4"), ("kStretch", "<f4"),
+                         ("connectionIndex", "<i4"), ("flags", "<u4")])
+
+
+def default_meta(n, maxH=1e-3):
+    """Sim::Sim defaults, YarnBall.cu:14-35."""
+    m = OrcMeta()
+    m.gravity[:] = [0.0, -9.8, 0.0]
+    m.numVerts = n
+    m.h = maxH
+    m.drag = 0.2
+    m.damping = 1e-6
+    m.radius = 1e-4
+    m.barrierThickness = 8e-4
+    m.accelerationRatio = 1.0
+    m.kCollision = 1e-5
+    m.detectionScaler = 1.2
+    m.frictionCoeff = 0.1
+    m.kFriction = 5.0
+    m.detectionPeriod = 1
+    m.useStepSizeLimit = 1
+    m.useVelocityRadius = 1
+    m.bvhRebuildPeriod = 0.1
+    m.numItr = 8
+    return m
+
+
+def default_vertices(n):
+    """Per-vertex defaults of Sim::Sim (YarnBall.cu:42-50)."""
+    v = np.zeros(n, VERTEX_DTYPE)
+    v["invMass"] = 1.0
+    v["lRest"] = 1.0
+    v["kStretch"] = 100.0
+    v["connectionIndex"] = -1
+    v["flags"] = 2
+    v["flags"][-1] = 0
+    q = np.zeros((n, 4), np.float32)
+    q[:, 3] = 1.0
+    qr = np.zeros((n, 4), np.float32)
+    qr[:, 3] = 5.0
+    return v, q, qr
+
+
+def build_scenes(pos_list, yarn_lengths_list, kbend_list, meta_fields, kstretch=2e-2, density=1e-3, mode=FP32,
+                 pin_first=True):
+    """Scenes assembled entirely on the oracle side (its own configure restatement): each
+    scene is a list of yarn polylines; returns an OracleSim holding all of them."""
+    verts, qs, qrs, metas, scene_of = [], [], [], [], []
+    for s, (pos, lens, kb) in enumerate(zip(pos_list, yarn_lengths_list, kbend_list)):
+        n = len(pos)
+        v, q, qr = default_vertices(n)
+        v["pos"] = pos
+        ends = np.cumsum(lens) - 1
+        v["flags"][ends] = 0
+        if pin_first:
+            v["invMass"][ends - np.asarray(lens) + 1] = 0.0
+        m = default_meta(n)
+        for k, val in meta_fields.items():
+            setattr(m, k, val)
+        st, v, q, qr, _, mx, mn = configure(v, q, qr, density)
+        if st != 0:
+            raise RuntimeError("oracle configure failed for scene %d (%d)" % (s, st))
+        m.maxSegLen, m.minSegLen = mx, mn
+        set_kbend(v, qr, kb)
+        set_kstretch(v, kstretch)
+        if load().orc_upload_meta(ctypes.addressof(m)) != 0:
+            raise RuntimeError("invalid parameters for scene %d" % s)
+        verts.append(v); qs.append(q); qrs.append(qr); metas.append(m)
+        scene_of.append(np.full(n, s, np.int32))
+    vall = np.concatenate(verts)
+    return OracleSim(vall, np.zeros((len(vall), 3), np.float32), np.concatenate(qs), np.concatenate(qrs), metas,
+                     mode=mode, scene_of=np.concatenate(scene_of) if len(metas) > 1 else None)
+
+
 def from_sim(sim, mode=FP64, **kw):
     """Oracle state from a yarnball_b200 Sim's host arrays and parameters (after configure)."""
     metas = [sim.scene_meta(s).as_struct() for s in range(sim.numScenes)]

@@ -131,7 +131,8 @@ def test_pile_small_substep_vs_fp64():
 
 
 def test_batched_equals_alone():
-    spec = scenes.batched_spec(seed=5, num_scenes=4, cap=40000)
+    spec = scenes.batched_spec(seed=5, num_scenes=5, cap=200000, max_yarns=12, min_len=32, max_len=400)
+    assert len(spec[0]) == 5
     batch, spec = scenes.build_batched(seed=5, spec=spec)
     batch.advance(1 / 30.0)
     pos_b, _, q_b = batch.read_state_f64()

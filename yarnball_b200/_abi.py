@@ -105,6 +105,8 @@ SIGNATURES = {
     "yb_set_tuning": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32]),
     "yb_get_tuning": (ctypes.c_int, [_P, c_int32_p, c_int32_p]),
     "yb_launch_count": (ctypes.c_int, [_P, c_uint64_p]),
+    "yb_set_stream": (ctypes.c_int, [_P, _P]),
+    "yb_profile_advance": (ctypes.c_int, [_P, ctypes.c_float, c_double_p, c_uint64_p]),
     "yb_info": (ctypes.c_int, [_P, c_int32_p, c_int32_p, c_int32_p]),
     "yb_penetration_count": (ctypes.c_int, [_P, c_int64_p]),
     "yb_diagnostics": (ctypes.c_int, [_P, c_double_p]),

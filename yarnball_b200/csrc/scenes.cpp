@@ -10,7 +10,8 @@
 //     components reflected (so every segment keeps length segLen);
 //   * a step is rejected when the new segment comes closer than minDist to any existing
 //     segment other than its two predecessors on the same yarn (uniform-grid search);
-//     after maxTries rejections in a row the yarn is discarded and restarted.
+//     after maxTries rejections in a row the walk backtracks, and a yarn that keeps failing
+//     is discarded and restarted.
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -102,7 +103,9 @@ struct Grid {
     }
 };
 
-// Generates one scene; returns 0 or -1 when a yarn could not be placed.
+// Generates one scene; returns 0 or -1 when a yarn could not be placed.  When a step
+// fails maxTries times in a row the walk backtracks (drops its last few vertices, more
+// on repeated failures) before giving up on the yarn and restarting it.
 int walk_scene(uint64_t seed, int numYarns, const int* vertsPerYarn, double segLen, double cube, double sigma,
                double minDist, int maxTries, int maxRestarts, float* out) {
     Rng rng(seed);
@@ -110,6 +113,7 @@ int walk_scene(uint64_t seed, int numYarns, const int* vertsPerYarn, double segL
     g.cell = segLen + minDist;
     std::vector<D3> s0, s1;   // segment endpoints
     std::vector<int> yarnOf;  // owning yarn attempt id
+    std::vector<int> segPos;  // index of the segment within its yarn
     std::vector<char> alive;
     size_t o = 0;
     int attemptId = 0;
@@ -118,14 +122,19 @@ int walk_scene(uint64_t seed, int numYarns, const int* vertsPerYarn, double segL
         bool placed = false;
         for (int restart = 0; restart <= maxRestarts && !placed; restart++) {
             const int id = attemptId++;
-            const size_t firstSeg = s0.size();
-            std::vector<D3> pts;
+            std::vector<D3> pts, dirs;
+            std::vector<int> segIds;  // global segment id of segment v-1 (ending at vertex v)
             pts.reserve(m);
             D3 p{cube * rng.uniform(), cube * rng.uniform(), cube * rng.uniform()};
             D3 dir = unit(D3{rng.normal(), rng.normal(), rng.normal()});
             pts.push_back(p);
+            dirs.push_back(dir);
+            int backtracks = 0, depth = 4;
             bool ok = true;
-            for (int v = 1; v < m && ok; v++) {
+            while ((int)pts.size() < m) {
+                const int v = (int)pts.size();
+                p = pts.back();
+                dir = dirs.back();
                 bool stepOk = false;
                 for (int t = 0; t < maxTries && !stepOk; t++) {
                     const double th = sigma * rng.normal();
@@ -148,7 +157,7 @@ int walk_scene(uint64_t seed, int numYarns, const int* vertsPerYarn, double segL
                         if (it == g.cells.end()) return;
                         for (int sidx : it->second) {
                             if (!alive[sidx]) continue;
-                            if (yarnOf[sidx] == id && (int)(sidx - firstSeg) >= segIdx - 2) continue;
+                            if (yarnOf[sidx] == id && segPos[sidx] >= segIdx - 2) continue;
                             if (seg_dist(p, q, s0[sidx], s1[sidx]) < minDist) {
                                 clash = true;
                                 return;
@@ -160,14 +169,30 @@ int walk_scene(uint64_t seed, int numYarns, const int* vertsPerYarn, double segL
                     s0.push_back(p);
                     s1.push_back(q);
                     yarnOf.push_back(id);
+                    segPos.push_back(segIdx);
                     alive.push_back(1);
                     g.for_cells(p, q, 0.0, [&](uint64_t k) { g.cells[k].push_back(sidx); });
-                    p = q;
-                    dir = nd;
-                    pts.push_back(p);
+                    pts.push_back(q);
+                    dirs.push_back(nd);
+                    segIds.push_back(sidx);
                     stepOk = true;
                 }
-                if (!stepOk) ok = false;
+                if (!stepOk) {
+                    if (++backtracks > 400) {
+                        ok = false;
+                        break;
+                    }
+                    const int drop = std::min((int)pts.size() - 1, depth);
+                    for (int k = 0; k < drop; k++) {
+                        alive[segIds.back()] = 0;
+                        segIds.pop_back();
+                        pts.pop_back();
+                        dirs.pop_back();
+                    }
+                    depth = std::min(depth * 2, 256);
+                } else if (depth > 4 && (int)pts.size() % 64 == 0) {
+                    depth /= 2;
+                }
             }
             if (ok) {
                 placed = true;
@@ -178,7 +203,7 @@ int walk_scene(uint64_t seed, int numYarns, const int* vertsPerYarn, double segL
                 }
                 o += m;
             } else {
-                for (size_t sidx = firstSeg; sidx < s0.size(); sidx++) alive[sidx] = 0;
+                for (int sidx : segIds) alive[sidx] = 0;
             }
         }
         if (!placed) return -1;

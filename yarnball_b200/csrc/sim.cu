@@ -49,6 +49,7 @@ struct EngineBase {
     virtual yb_status diagnostics(double* out) = 0;
     virtual uint64_t debug_phases(int mask, int& buf) = 0;
     virtual int64_t penetrations() = 0;
+    virtual yb_status profile_substep(bool detect, bool rebuild, double* ms, uint64_t* launches) = 0;
 };
 
 }  // namespace
@@ -73,7 +74,8 @@ struct yb_sim {
     int iterBlock = 256;
     int useGraphs = 1;
     uint64_t launches = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;     // active stream (own or the caller's)
+    cudaStream_t ownStream = nullptr;  // created by configure, destroyed by yb_destroy
     EngineBase* eng = nullptr;
     int dbgBuf = 0;
     std::vector<int> segs;  // host copy of the segment list
@@ -591,6 +593,55 @@ struct Engine : EngineBase {
         return YB_OK;
     }
 
+    // One substep with each kernel class bracketed by events (see yb_profile_advance).
+    yb_status profile_substep(bool detect, bool rebuild, double* ms, uint64_t* launches) override {
+        cudaStream_t st = S->stream;
+        cudaEvent_t ev[16];
+        int cls[16];
+        int ne = 0;
+        for (auto& e : ev) YB_CUDA(cudaEventCreate(&e));
+        auto mark = [&](int c) {
+            cls[ne] = c;
+            cudaEventRecord(ev[ne++], st);
+        };
+        const int I = num_itr();
+        mark(0);
+        launch_init(d, st); launches[0]++;
+        if (detect && d.nseg > 0) {
+            if (rebuild) {
+                mark(1);
+                launch_bvh_rebuild(d, st, sortScratch, sortBytes, keyBits);
+                const int passes = d.nseg > 1 ? (keyBits + 7) / 8 : 0;
+                launches[1] += 3 + (d.nseg > 1 ? 2 + passes : 0) + 1 + (d.nseg > 1 ? 1 : 0);
+            } else {
+                mark(2);
+                launch_bvh_refit(d, st);
+                launches[2] += d.nseg > 1 ? 1 : 0;
+            }
+            mark(3);
+            launch_traverse(d, st); launches[3]++;
+        } else {
+            mark(4);
+            launch_step_limit(d, st); launches[4]++;
+        }
+        mark(5);
+        for (int it = 0; it < I; it++) launch_iter(d, it & 1, S->iterBlock, st);
+        launches[5] += I;
+        mark(6);
+        launch_end(d, I & 1, (I & 1) != 0, sizeof(R) == 4, st); launches[6]++;
+        mark(-1);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaEventSynchronize(ev[ne - 1]);
+        for (int i = 0; e == cudaSuccess && i + 1 < ne; i++) {
+            float t = 0.f;
+            e = cudaEventElapsedTime(&t, ev[i], ev[i + 1]);
+            ms[cls[i]] += t;
+        }
+        for (auto& x : ev) cudaEventDestroy(x);
+        S->launches += 0;
+        return cuda_status(e);
+    }
+
     uint64_t debug_phases(int mask, int& buf) override {
         cudaStream_t st = S->stream;
         uint64_t k = 0;
@@ -692,7 +743,10 @@ void yb_destroy(yb_sim* S) {
     if (!S) return;
     if (S->stream) cudaStreamSynchronize(S->stream);
     delete S->eng;
-    if (S->stream) cudaStreamDestroy(S->stream);
+    if (S->ownStream) {
+        cudaStreamSynchronize(S->ownStream);
+        cudaStreamDestroy(S->ownStream);
+    }
     if (S->pinned)
         cudaFreeHost(S->verts);
     else
@@ -751,13 +805,14 @@ yb_status yb_configure(yb_sim* S, float density) {
         S->eng = nullptr;
         S->configured = false;
     }
-    if (!S->stream) {
-        cudaError_t e = cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking);
+    if (!S->ownStream) {
+        cudaError_t e = cudaStreamCreateWithFlags(&S->ownStream, cudaStreamNonBlocking);
         if (e != cudaSuccess) {
-            S->stream = nullptr;
+            S->ownStream = nullptr;
             return cuda_status(e);
         }
     }
+    if (!S->stream) S->stream = S->ownStream;
     S->eng = make_engine(S);
     if (!S->eng) return YB_ERR_OUT_OF_MEMORY;
     yb_status st = engine_alloc(S);
@@ -934,6 +989,50 @@ yb_status yb_get_tuning(yb_sim* S, int32_t* iterBlock, int32_t* useGraphs) {
     if (iterBlock) *iterBlock = S->iterBlock;
     if (useGraphs) *useGraphs = S->useGraphs;
     return YB_OK;
+}
+
+yb_status yb_set_stream(yb_sim* S, void* stream) {
+    if (!S) return YB_ERR_INVALID_ARGUMENT;
+    if (S->stream) {
+        cudaError_t e = cudaStreamSynchronize(S->stream);
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    S->stream = stream ? (cudaStream_t)stream : S->ownStream;
+    return YB_OK;
+}
+
+yb_status yb_profile_advance(yb_sim* S, float dt, double* msByClass, uint64_t* launchesByClass) {
+    if (!S || !msByClass || !launchesByClass) return YB_ERR_INVALID_ARGUMENT;
+    if (!S->configured) return YB_ERR_NOT_CONFIGURED;
+    if (!(dt > 0)) return YB_OK;
+    const int steps = std::max(1, (int)std::ceil(dt / S->maxH));
+    for (auto& m : S->meta) {
+        m.lastH = m.h;
+        m.h = dt / steps;
+    }
+    yb_status st = validate_all_meta(S);
+    if (st != YB_OK) return st;
+    S->eng->write_params();
+    const yb_meta& m0 = S->meta[0];
+    for (int s = 0; s < steps; s++, S->stepCounter++) {
+        bool detect = false, rebuild = false;
+        if (m0.detectionPeriod > 0 && S->stepCounter % (uint64_t)m0.detectionPeriod == 0) {
+            detect = true;
+            if (S->lastBVHRebuild >= m0.bvhRebuildPeriod) {
+                rebuild = true;
+                S->lastBVHRebuild = 0;
+            } else {
+                S->lastBVHRebuild += m0.h * m0.detectionPeriod;
+            }
+        }
+        uint64_t before[YB_PROFILE_CLASSES];
+        std::memcpy(before, launchesByClass, sizeof(before));
+        st = S->eng->profile_substep(detect, rebuild, msByClass, launchesByClass);
+        for (int c = 0; c < YB_PROFILE_CLASSES; c++) S->launches += launchesByClass[c] - before[c];
+        if (st != YB_OK) return st;
+    }
+    for (auto& m : S->meta) m.time += dt;
+    return S->eng->check_errors();
 }
 
 yb_status yb_launch_count(yb_sim* S, uint64_t* out) {

@@ -181,16 +181,17 @@ class TwistDriver:
         self.t += dt
 
 
-def batched_spec(seed=7, num_scenes=512, cap=8388608):
-    """Scene sizes of the batched workload: k ~ U{1..64} yarns per scene, vertices per yarn
-    log-uniform in [64, 4096], kBend log-uniform in [1e-9, 1e-7]; scenes are added until the
-    next one would exceed `cap` vertices.  Draws use numpy's PCG64 seeded with `seed`."""
+def batched_spec(seed=7, num_scenes=512, cap=8388608, max_yarns=64, min_len=64, max_len=4096):
+    """Scene sizes of the batched workload: k ~ U{1..max_yarns} yarns per scene, vertices per
+    yarn log-uniform in [min_len, max_len], kBend log-uniform in [1e-9, 1e-7]; scenes are
+    added until the next one would exceed `cap` vertices.  Draws use numpy's PCG64 seeded
+    with `seed`."""
     rng = np.random.Generator(np.random.PCG64(seed))
     yarns, lens, kbend = [], [], []
     total = 0
     for _ in range(num_scenes):
-        k = int(rng.integers(1, 65))
-        ls = np.exp(rng.uniform(math.log(64), math.log(4096), size=k)).astype(np.int32)
+        k = int(rng.integers(1, max_yarns + 1))
+        ls = np.exp(rng.uniform(math.log(min_len), math.log(max_len), size=k)).astype(np.int32)
         kb = float(10 ** rng.uniform(-9, -7))
         if total + int(ls.sum()) > cap:
             break

@@ -209,6 +209,20 @@ class Sim:
     def set_tuning(self, iterBlock=256, useGraphs=True):
         check(self._lib.yb_set_tuning(self._h, int(iterBlock), 1 if useGraphs else 0), "tuning")
 
+    def set_stream(self, stream_handle):
+        """Launch on a caller's cudaStream_t (int handle, e.g. torch's stream.cuda_stream); 0 = own."""
+        check(self._lib.yb_set_stream(self._h, ctypes.c_void_p(int(stream_handle) or None)), "set_stream")
+
+    PROFILE_CLASSES = ["init", "bvh_rebuild", "bvh_refit", "traverse", "step_limit", "iter", "end"]
+
+    def profile_advance(self, dt):
+        """advance(dt) with per-kernel-class device times (ms) and launch counts."""
+        ms = np.zeros(7, np.float64)
+        ln = np.zeros(7, np.uint64)
+        check(self._lib.yb_profile_advance(self._h, float(dt), ptr(ms, ctypes.c_double), ptr(ln, ctypes.c_uint64)),
+              "profile_advance")
+        return dict(zip(self.PROFILE_CLASSES, ms.tolist())), dict(zip(self.PROFILE_CLASSES, ln.tolist()))
+
     def launch_count(self):
         v = ctypes.c_uint64()
         check(self._lib.yb_launch_count(self._h, ctypes.byref(v)))
