@@ -230,6 +230,32 @@ def default_vertices(n):
     return v, q, qr
 
 
+def prepare_scene(pos, lens, kbend, meta_fields, kstretch=2e-2, density=1e-3, pin_first=True, pin_last=False):
+    """One scene of yarn polylines set up as the reference host code does (defaults,
+    configure, setKBend, setKStretch, uploadMeta); returns (verts, qs, qRests, meta)."""
+    n = len(pos)
+    v, q, qr = default_vertices(n)
+    v["pos"] = pos
+    ends = np.cumsum(lens) - 1
+    v["flags"][ends] = 0
+    if pin_first:
+        v["invMass"][ends - np.asarray(lens) + 1] = 0.0
+    if pin_last:
+        v["invMass"][ends] = 0.0
+    m = default_meta(n)
+    for k, val in meta_fields.items():
+        setattr(m, k, val)
+    st, v, q, qr, _, mx, mn = configure(v, q, qr, density)
+    if st != 0:
+        raise RuntimeError("oracle configure failed (%d)" % st)
+    m.maxSegLen, m.minSegLen = mx, mn
+    set_kbend(v, qr, kbend)
+    set_kstretch(v, kstretch)
+    if load().orc_upload_meta(ctypes.addressof(m)) != 0:
+        raise RuntimeError("invalid scene parameters")
+    return v, q, qr, m
+
+
 def build_scenes(pos_list, yarn_lengths_list, kbend_list, meta_fields, kstretch=2e-2, density=1e-3, mode=FP32,
                  pin_first=True):
     """Scenes assembled entirely on the oracle side (its own configure restatement): each
@@ -237,23 +263,7 @@ def build_scenes(pos_list, yarn_lengths_list, kbend_list, meta_fields, kstretch=
     verts, qs, qrs, metas, scene_of = [], [], [], [], []
     for s, (pos, lens, kb) in enumerate(zip(pos_list, yarn_lengths_list, kbend_list)):
         n = len(pos)
-        v, q, qr = default_vertices(n)
-        v["pos"] = pos
-        ends = np.cumsum(lens) - 1
-        v["flags"][ends] = 0
-        if pin_first:
-            v["invMass"][ends - np.asarray(lens) + 1] = 0.0
-        m = default_meta(n)
-        for k, val in meta_fields.items():
-            setattr(m, k, val)
-        st, v, q, qr, _, mx, mn = configure(v, q, qr, density)
-        if st != 0:
-            raise RuntimeError("oracle configure failed for scene %d (%d)" % (s, st))
-        m.maxSegLen, m.minSegLen = mx, mn
-        set_kbend(v, qr, kb)
-        set_kstretch(v, kstretch)
-        if load().orc_upload_meta(ctypes.addressof(m)) != 0:
-            raise RuntimeError("invalid parameters for scene %d" % s)
+        v, q, qr, m = prepare_scene(pos, lens, kb, meta_fields, kstretch, density, pin_first)
         verts.append(v); qs.append(q); qrs.append(qr); metas.append(m)
         scene_of.append(np.full(n, s, np.int32))
     vall = np.concatenate(verts)
