@@ -42,7 +42,8 @@ typedef enum yb_status {
     YB_ERR_CUDA = 9,                   /* replaces checkCudaErrors' exit(), Common.h:15-21 */
     YB_ERR_OUT_OF_MEMORY = 10,
     YB_ERR_INTERNAL = 11,              /* a bounded device wait expired or the BVH stack overflowed */
-    YB_ERR_ALREADY_CONFIGURED = 12
+    YB_ERR_ALREADY_CONFIGURED = 12,
+    YB_ERR_SCRATCH_TOO_SMALL = 13      /* request larger than a fixed scratch area */
 } yb_status;
 
 /* VertexFlags, YarnBall.h:34-40 */
@@ -225,6 +226,22 @@ yb_status yb_debug_phases(yb_sim* sim, int32_t mask, float h);
  * the BVH build (ascending by the low `bits` key bits). */
 yb_status yb_debug_sort_pairs(const uint64_t* keys, const int32_t* vals, int32_t n, int32_t bits,
                               uint64_t* keysOut, int32_t* valsOut);
+
+/* Allocation-free variant of the sort above (no counterpart in the reference).  For callers
+ * that may not allocate device memory where they sort - code running inside another
+ * framework that owns the device-memory budget through its own pool, or a fixed-budget loop
+ * in which an allocation (which can synchronise the device or fail under fragmentation) is
+ * an error.  keysIn/valsIn/keysOut/valsOut are DEVICE pointers owned by the caller (inputs
+ * are only read); stream is a cudaStream_t (NULL = legacy default).  Scratch is a fixed
+ * array compiled into the library (about 4.2 MB held on every GPU that loads it), so n is
+ * limited to YB_SORT_NOALLOC_MAX_N; larger n returns YB_ERR_SCRATCH_TOO_SMALL.  No
+ * cudaMalloc/cudaFree or allocating library call is made.  The first call on a device looks
+ * the scratch address up (make it before any stream capture).  Calls share the scratch:
+ * calls that overlap on the GPU race and must be serialised.  Returns after the sort has
+ * completed on `stream`. */
+#define YB_SORT_NOALLOC_MAX_N 262144
+yb_status yb_sort_pairs_noalloc(const uint64_t* keysIn, const int32_t* valsIn, uint64_t* keysOut,
+                                int32_t* valsOut, int32_t n, int32_t bits, void* stream);
 
 #ifdef __cplusplus
 }

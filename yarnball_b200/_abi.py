@@ -116,6 +116,7 @@ SIGNATURES = {
     "yb_debug_phases": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_float]),
     "yb_debug_sort_pairs": (ctypes.c_int, [c_uint64_p, c_int32_p, ctypes.c_int32, ctypes.c_int32, c_uint64_p,
                                            c_int32_p]),
+    "yb_sort_pairs_noalloc": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int32, ctypes.c_int32, _P]),
     "yb_scene_random_walks": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_int32, c_int32_p, ctypes.c_float,
                                              ctypes.c_float, ctypes.c_float, ctypes.c_float, c_float_p]),
     "yb_scene_random_walks_batch": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_int32, c_int32_p, c_int32_p,

@@ -10,7 +10,10 @@
 // Tiles only wait on tiles that obtained a smaller index from the counter, i.e. that are
 // already running, so the look-back always completes; every wait is still bounded and a
 // timeout sets IE_SORT_WAIT in the error word instead of hanging.
+#include <mutex>
+
 #include "engine.cuh"
+#include "yarnball_b200.h"
 
 namespace yb {
 
@@ -185,3 +188,110 @@ int radix_sort_pairs(unsigned long long* keys[2], int* vals[2], int n, int bits,
 }
 
 }  // namespace yb
+
+// =========================================================================================
+// Allocation-free sort (yb_sort_pairs_noalloc).
+//
+// Some callers cannot allocate device memory at the point where they need a sort: code that
+// runs inside a host framework which owns the whole device-memory budget through its own
+// pool, or a fixed-budget simulation/render loop where an allocation (which may synchronise
+// the device, or fail once memory is fragmented) is treated as an error.  This variant uses
+// only the caller's input/output buffers plus one fixed scratch area compiled into the
+// library as a file-scope __device__ array.  Every GPU that loads the library holds that
+// array (about 4.2 MB) until the process exits.  The library looks its address up once per
+// device with cudaGetSymbolAddress (host code may not use the symbol itself as a device
+// address); that set-up happens inside the first call on each device, so make that first
+// call before any stream capture.  All calls share the array: calls whose GPU work overlaps
+// (two streams, or two host threads at once) race on it and must be serialised by the caller.
+namespace yb {
+namespace {
+
+constexpr int NOALLOC_MAX_N = 1 << 18;  // 262,144 pairs (YB_SORT_NOALLOC_MAX_N)
+constexpr int NOALLOC_TILES = (NOALLOC_MAX_N + SORT_TILE - 1) / SORT_TILE;
+constexpr int NOALLOC_WORDS = SORT_MAX_PASSES * 256 + SORT_MAX_PASSES + SORT_MAX_PASSES * NOALLOC_TILES * 256;
+
+struct NoAllocScratch {
+    unsigned long long keys[NOALLOC_MAX_N];
+    int vals[NOALLOC_MAX_N];
+    unsigned words[NOALLOC_WORDS];  // histograms | tile counters | look-back status words
+    int err;
+};
+
+static __device__ __align__(256) unsigned char g_sort_scratch[sizeof(NoAllocScratch)];
+
+constexpr int MAX_DEVICES = 256;
+std::mutex g_scratch_mu;
+void* g_scratch_addr[MAX_DEVICES] = {nullptr};
+
+// Device address of g_sort_scratch on the current device (looked up once per device).
+cudaError_t scratch_address(NoAllocScratch** out) {
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= MAX_DEVICES) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    if (!g_scratch_addr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_sort_scratch);
+        if (e != cudaSuccess) return e;
+        g_scratch_addr[dev] = p;
+    }
+    *out = (NoAllocScratch*)g_scratch_addr[dev];
+    return cudaSuccess;
+}
+
+}  // namespace
+}  // namespace yb
+
+extern "C" yb_status yb_sort_pairs_noalloc(const uint64_t* keysIn, const int32_t* valsIn, uint64_t* keysOut,
+                                           int32_t* valsOut, int32_t n, int32_t bits, void* stream) {
+    using namespace yb;
+    if (n < 0 || bits < 0 || bits > 64) return YB_ERR_INVALID_ARGUMENT;
+    if (n > NOALLOC_MAX_N) return YB_ERR_SCRATCH_TOO_SMALL;
+    if (n == 0) return YB_OK;
+    if (!keysIn || !valsIn || !keysOut || !valsOut) return YB_ERR_INVALID_ARGUMENT;
+    NoAllocScratch* S = nullptr;
+    cudaError_t e = scratch_address(&S);
+    if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? YB_ERR_OUT_OF_MEMORY : YB_ERR_CUDA;
+    cudaStream_t st = (cudaStream_t)stream;
+    const unsigned long long* kin = (const unsigned long long*)keysIn;
+    unsigned long long* kout = (unsigned long long*)keysOut;
+    const int passes = n == 1 ? 0 : (bits + 7) / 8;
+    if (passes == 0) {
+        e = cudaMemcpyAsync(kout, kin, sizeof(unsigned long long) * n, cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(valsOut, valsIn, sizeof(int) * n, cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        return e == cudaSuccess ? YB_OK : YB_ERR_CUDA;
+    }
+    const int tiles = sort_tiles(n);
+    unsigned* hist = S->words;
+    unsigned* counters = hist + SORT_MAX_PASSES * 256;
+    unsigned* status = counters + SORT_MAX_PASSES;
+    // The scratch keeps the previous call's contents: clear what must start at zero.
+    e = cudaMemsetAsync(S->words, 0, sizeof(unsigned) * (SORT_MAX_PASSES * 256 + SORT_MAX_PASSES), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(status, 0, sizeof(unsigned) * (size_t)passes * tiles * 256, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(&S->err, 0, sizeof(int), st);
+    if (e != cudaSuccess) return YB_ERR_CUDA;
+    int hb = (n + SORT_THREADS * 4 - 1) / (SORT_THREADS * 4);
+    k_sort_hist<<<hb, SORT_THREADS, 0, st>>>(kin, n, passes, hist);
+    k_sort_scan<<<1, 256, 0, st>>>(hist, passes);
+    // Pass p writes the output buffers when (passes-1-p) is even and the scratch otherwise,
+    // so the last pass lands in the caller's output; pass 0 reads the caller's input.
+    const unsigned long long* srcK = kin;
+    const int* srcV = valsIn;
+    for (int p = 0; p < passes; p++) {
+        const bool toOut = ((passes - 1 - p) & 1) == 0;
+        unsigned long long* dstK = toOut ? kout : S->keys;
+        int* dstV = toOut ? valsOut : S->vals;
+        k_sort_pass<<<tiles, SORT_THREADS, 0, st>>>(srcK, srcV, dstK, dstV, n, 8 * p, hist + p * 256,
+                                                    status + (size_t)p * tiles * 256, counters + p, &S->err);
+        srcK = dstK;
+        srcV = dstV;
+    }
+    int herr = 0;
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, &S->err, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return YB_ERR_CUDA;
+    return herr ? YB_ERR_INTERNAL : YB_OK;
+}

@@ -971,6 +971,8 @@ const char* yb_status_string(yb_status s) {
         case YB_ERR_OUT_OF_MEMORY: return "out of device or host memory";
         case YB_ERR_INTERNAL: return "internal error: a bounded device wait expired or the BVH stack overflowed";
         case YB_ERR_ALREADY_CONFIGURED: return "already configured";
+        case YB_ERR_SCRATCH_TOO_SMALL:
+            return "request exceeds the fixed scratch area of the allocation-free entry point (n > YB_SORT_NOALLOC_MAX_N)";
     }
     return "unknown status";
 }
