@@ -241,6 +241,10 @@ def run_ours(args):
     sim.set_stream(stream.cuda_stream)
     for _ in range(args.warmup):
         sim.advance(FRAME)
+    # Autotuner: Newton-kernel shape (threads per block, lanes per vertex) timed on this state.
+    tune_threads, tune_lanes, tune_ms = sim.autotune()
+    cfg["newton_kernel_shape"] = {"threads": tune_threads, "lanes_per_vertex": tune_lanes,
+                                  "autotune_ms_per_launch": tune_ms}
     try:
         uuid = str(torch.cuda.get_device_properties(local).uuid)
         gpu_id = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
@@ -331,7 +335,7 @@ def run_ours(args):
     pens = sim.penetrations()
     plain = None
     if not args.no_plain and rank == 0 and world == 1:
-        plain = run_plain(spec, stream)
+        plain = run_plain(spec, stream, (tune_threads, tune_lanes))
     sim.close()
     cpu = None
     if not args.no_cpu and rank == 0 and world == 1:
@@ -355,7 +359,7 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def run_plain(spec, stream):
+def run_plain(spec, stream, shape):
     """The drop-in path: one Sim per scene, advance() called scene after scene."""
     import torch
 
@@ -378,6 +382,7 @@ def run_plain(spec, stream):
         sm.maxH = MAX_H
         sm.upload()
         sm.set_stream(stream.cuda_stream)
+        sm.set_tuning(shape[0], shape[1], True)
         sims.append(sm)
         off += counts[s]
     for sm in sims:

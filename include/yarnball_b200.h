@@ -174,10 +174,15 @@ const char* yb_status_string(yb_status s);
 
 /* ---- Additions without a reference counterpart ---------------------------------- */
 
-/* Engine tuning: Newton block size (64/128/256/512) and whether substeps replay captured
- * CUDA graphs.  Defaults come from the autotuner or 256 / graphs on. */
-yb_status yb_set_tuning(yb_sim* sim, int32_t iterBlock, int32_t useGraphs);
-yb_status yb_get_tuning(yb_sim* sim, int32_t* iterBlock, int32_t* useGraphs);
+/* Engine tuning: threads per block of the Newton kernel and lanes per vertex (lanes split a
+ * segment's contact loop: (128|256, 1), (256, 2), (256|512, 4), (256|512, 8)), and whether
+ * substeps replay captured CUDA graphs.  Default (256, 4), graphs on. */
+yb_status yb_set_tuning(yb_sim* sim, int32_t iterThreads, int32_t lanesPerVertex, int32_t useGraphs);
+yb_status yb_get_tuning(yb_sim* sim, int32_t* iterThreads, int32_t* lanesPerVertex, int32_t* useGraphs);
+
+/* Autotuner: times every Newton-kernel shape on the current device state (which it leaves
+ * unchanged), keeps the fastest and returns it.  Call after at least one advance(). */
+yb_status yb_autotune(yb_sim* sim, int32_t* bestThreads, int32_t* bestLanes, float* bestMs);
 
 /* Launch the simulation's work on `stream` (a cudaStream_t; NULL returns to the simulation's
  * own stream).  Lets a caller order the engine with its own work and time it with events. */

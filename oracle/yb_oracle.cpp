@@ -502,10 +502,15 @@ struct Sim : SimBase {
                     const T s = rdot(rmul(rinv(q0), qq), qr) > T(0) ? T(1) : T(-1);
                     b = radd(b, rscale(s, rmul(qq, rinv(qr))));
                 }
-                const T lambda = len(v) + rlen(b);
-                const rot<T> t = rmul(rmul(rot<T>{v.x, v.y, v.z, T(0)}, b), rot<T>{T(1), T(0), T(0), T(0)});
-                const rot<T> r = radd(t, rscale(lambda, b));
-                q0 = rscale(T(1) / rlen(r), r);
+                // b = 0 (a yarn of one segment) makes the closed form 0/0; the orientation
+                // is kept there (the reference's expression yields NaN).
+                const T bl = rlen(b);
+                if (bl > T(0)) {
+                    const T lambda = len(v) + bl;
+                    const rot<T> t = rmul(rmul(rot<T>{v.x, v.y, v.z, T(0)}, b), rot<T>{T(1), T(0), T(0), T(0)});
+                    const rot<T> r = radd(t, rscale(lambda, b));
+                    q0 = rscale(T(1) / rlen(r), r);
+                }
             }
             qn[i] = q0;
         }

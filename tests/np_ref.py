@@ -202,6 +202,8 @@ def substep(st, meta):
             if fl[i] & HAS_NEXT_ORI:
                 s = 1.0 if qmul(qinv(q[i]), q[i + 1]) @ qRest[i] > 0 else -1.0
                 b += s * qmul(q[i + 1], qinv(qRest[i]))
+            if np.linalg.norm(b) == 0:
+                continue  # one-segment yarn: the closed form is 0/0, orientation kept
             lam = np.linalg.norm(v) + np.linalg.norm(b)
             r = qmul(qmul(np.concatenate([v, [0.0]]), b), np.array([1.0, 0, 0, 0])) + lam * b
             nq[i] = r / np.linalg.norm(r)

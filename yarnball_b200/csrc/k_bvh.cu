@@ -208,42 +208,60 @@ __global__ void __launch_bounds__(256) k_refit(Dev<R> d, const int* __restrict__
 }
 
 constexpr int BVH_STACK = 64;
+constexpr int TRAV_THREADS = 128;
+constexpr int TRAV_WARPS = TRAV_THREADS / 32;
+constexpr int TRAV_QCAP = 96;       // < 32 left over + up to 2 candidates per lane
+constexpr int TRAV_JBITS = 26;      // candidate entry = (owner lane << 26) | partner segment
 
+// Appends y to x's contact list.  The count keeps growing past MAX_COLS so that the list
+// kernel can report the overflow (collision.cu:80-90).
 template <typename R>
-__global__ void __launch_bounds__(128) k_traverse(Dev<R> d) {
+__device__ __forceinline__ void list_append(const Dev<R>& d, int x, int y) {
+    const int pos = atomicAdd(&d.numCols[x], 1);
+    if (pos < MAX_COLS) d.cols[x + (size_t)d.n * pos] = y;
+}
+
+// Broadphase + narrow phase.  Each lane walks its own segment's scene subtree; a leaf whose
+// box overlaps and whose segment index is larger than the query's becomes a candidate pair
+// in a per-warp queue.  Whenever 32 candidates are queued, the whole warp runs the
+// separately rounded narrow-phase test on them, one pair per lane, so the expensive test
+// never runs with idle lanes; kept pairs are appended to both segments' lists.
+template <typename R>
+__global__ void __launch_bounds__(TRAV_THREADS) k_traverse(Dev<R> d) {
+    __shared__ int sQ[TRAV_WARPS][TRAV_QCAP];
+    __shared__ int sSeg[TRAV_WARPS][32];
+    __shared__ int sScene[TRAV_WARPS][32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int si = blockIdx.x * blockDim.x + threadIdx.x;
-    if (si >= d.nseg) return;
-    const int k = d.segs[si];
-    const uint32_t flags = d.vp[k].flags;
-    const int sc = scene_of(flags);
-    const SceneParams<R>& sp = d.sp[sc];
-    const Box<R> qb = segment_box(d, k, sp);
-    const size_t n = (size_t)d.n;
-    int* __restrict__ cl = d.cols + k;
-    int cnt = 0;
-    int node = d.sceneRoot[sc];
-    if (node >= 0) {
-        int stack[BVH_STACK];
-        int top = 0;
-        while (true) {
+    int k = -1, node = -1, sc = 0;
+    Box<R> qb;
+    if (si < d.nseg) {
+        k = d.segs[si];
+        sc = scene_of(d.vp[k].flags);
+        qb = segment_box(d, k, d.sp[sc]);
+        node = d.sceneRoot[sc];
+    }
+    sSeg[warp][lane] = k;
+    sScene[warp][lane] = sc;
+    bool done = node < 0;  // leaf root (one segment) or no query
+    int stack[BVH_STACK];
+    int top = 0;
+    int qn = 0;  // queued candidates (identical in every lane)
+    const unsigned lt = (1u << lane) - 1u;
+    __syncwarp();
+    while (true) {
+        int c0 = -1, c1 = -1;
+        if (!done) {
             const BNode<R>& nd = d.nodes[node];
             bool ol = box_overlap(qb, nd.lmin, nd.lmax);
             bool orr = box_overlap(qb, nd.rmin, nd.rmax);
             const int L = nd.left, Rc = nd.right;
             if (ol && L < 0) {
-                const int j = -L - 1;
-                if (j != k && pair_keep(d, min(j, k), max(j, k), sp)) {
-                    if (cnt < MAX_COLS) cl[n * cnt] = j;
-                    cnt++;
-                }
+                if (-L - 1 > k) c0 = -L - 1;
                 ol = false;
             }
             if (orr && Rc < 0) {
-                const int j = -Rc - 1;
-                if (j != k && pair_keep(d, min(j, k), max(j, k), sp)) {
-                    if (cnt < MAX_COLS) cl[n * cnt] = j;
-                    cnt++;
-                }
+                if (-Rc - 1 > k) c1 = -Rc - 1;
                 orr = false;
             }
             if (ol && orr) {
@@ -257,26 +275,66 @@ __global__ void __launch_bounds__(128) k_traverse(Dev<R> d) {
                 node = L;
             } else if (orr) {
                 node = Rc;
-            } else {
-                if (top == 0) break;
+            } else if (top > 0) {
                 node = stack[--top];
+            } else {
+                done = true;
             }
         }
-    }
-    if (cnt > MAX_COLS) d.err[EW_ERROR] = 1;
-    const int nc = min(cnt, MAX_COLS);
-    if (nc) atomicMax(&d.err[EW_MAX_COLS], cnt);
-    // Insertion sort of the list by partner id (fixed summation order in the iteration).
-    for (int a = 1; a < nc; a++) {
-        const int v = cl[n * a];
-        int b = a - 1;
-        while (b >= 0 && cl[n * b] > v) {
-            cl[n * (b + 1)] = cl[n * b];
-            b--;
+        const unsigned b0 = __ballot_sync(0xffffffffu, c0 >= 0);
+        const unsigned b1 = __ballot_sync(0xffffffffu, c1 >= 0);
+        if (c0 >= 0) sQ[warp][qn + __popc(b0 & lt)] = (lane << TRAV_JBITS) | c0;
+        if (c1 >= 0) sQ[warp][qn + __popc(b0) + __popc(b1 & lt)] = (lane << TRAV_JBITS) | c1;
+        qn += __popc(b0) + __popc(b1);
+        __syncwarp();
+        const bool allDone = __all_sync(0xffffffffu, done);
+        while (qn >= 32 || (allDone && qn > 0)) {
+            const int m = min(qn, 32);
+            if (lane < m) {
+                const int e = sQ[warp][qn - m + lane];
+                const int owner = e >> TRAV_JBITS;
+                const int j = e & ((1 << TRAV_JBITS) - 1);
+                const int x = sSeg[warp][owner];
+                if (pair_keep(d, x, j, d.sp[sScene[warp][owner]])) {
+                    list_append(d, x, j);
+                    list_append(d, j, x);
+                }
+            }
+            qn -= m;
+            __syncwarp();
         }
-        cl[n * (b + 1)] = v;
+        if (allDone && qn == 0) break;
     }
-    d.numCols[k] = nc;
+}
+
+// Per segment after the broadphase: clamp and check the count, sort the list by partner id
+// (fixed summation order in the Newton iteration), then the step-size limit.  With
+// sortLists = 0 it only recomputes the step limit from the existing lists (substeps without
+// detection, collision.cu:121-172).
+template <typename R>
+__global__ void __launch_bounds__(128) k_lists(Dev<R> d, int sortLists) {
+    const int si = blockIdx.x * blockDim.x + threadIdx.x;
+    if (si >= d.nseg) return;
+    const int k = d.segs[si];
+    const SceneParams<R>& sp = d.sp[scene_of(d.vp[k].flags)];
+    int nc = d.numCols[k];
+    if (sortLists) {
+        if (nc > MAX_COLS) d.err[EW_ERROR] = 1;
+        if (nc) atomicMax(&d.err[EW_MAX_COLS], nc);
+        nc = min(nc, MAX_COLS);
+        const size_t n = (size_t)d.n;
+        int* __restrict__ cl = d.cols + k;
+        for (int a = 1; a < nc; a++) {
+            const int v = cl[n * a];
+            int b = a - 1;
+            while (b >= 0 && cl[n * b] > v) {
+                cl[n * (b + 1)] = cl[n * b];
+                b--;
+            }
+            cl[n * (b + 1)] = v;
+        }
+        d.numCols[k] = nc;
+    }
     d.stepLim[k] = segment_step_limit(d, k, sp, nc);
 }
 
@@ -314,7 +372,15 @@ void launch_bvh_refit(const Dev<R>& d, cudaStream_t s) {
 template <typename R>
 void launch_traverse(const Dev<R>& d, cudaStream_t s) {
     if (d.nseg <= 0) return;
-    k_traverse<R><<<(d.nseg + 127) / 128, 128, 0, s>>>(d);
+    cudaMemsetAsync(d.numCols, 0, sizeof(int) * d.n, s);
+    k_traverse<R><<<(d.nseg + TRAV_THREADS - 1) / TRAV_THREADS, TRAV_THREADS, 0, s>>>(d);
+    k_lists<R><<<(d.nseg + 127) / 128, 128, 0, s>>>(d, 1);
+}
+
+template <typename R>
+void launch_lists_step_limit(const Dev<R>& d, cudaStream_t s) {
+    if (d.nseg <= 0) return;
+    k_lists<R><<<(d.nseg + 127) / 128, 128, 0, s>>>(d, 0);
 }
 
 template void launch_bvh_rebuild<float>(const Dev<float>&, cudaStream_t, void*, size_t, int);
@@ -324,6 +390,8 @@ template void launch_bvh_refit<double>(const Dev<double>&, cudaStream_t);
 template void launch_bvh_reset<float>(const Dev<float>&, cudaStream_t);
 template void launch_bvh_reset<double>(const Dev<double>&, cudaStream_t);
 template void launch_traverse<float>(const Dev<float>&, cudaStream_t);
+template void launch_lists_step_limit<float>(const Dev<float>&, cudaStream_t);
+template void launch_lists_step_limit<double>(const Dev<double>&, cudaStream_t);
 template void launch_traverse<double>(const Dev<double>&, cudaStream_t);
 
 }  // namespace yb

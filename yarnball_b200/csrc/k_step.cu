@@ -1,12 +1,10 @@
-// k_step.cu - predictor, fused block-Jacobi Newton + orientation iteration, advection,
-// and the per-segment step-size limit.
+// k_step.cu - predictor, fused block-Jacobi Newton + orientation iteration, advection.
 //
 // Reference semantics (file:line in the reference project):
 //   initItr               KittenEngine/YarnBall/sim/iteration.cu:7-41
 //   cosseratItr           KittenEngine/YarnBall/sim/cosserat.cu:20-207
 //   quaternionLambdaItr   KittenEngine/YarnBall/sim/cosserat.cu:209-253
 //   endItr                KittenEngine/YarnBall/sim/iteration.cu:48-61
-//   recomputeStepLimit    KittenEngine/YarnBall/sim/collision.cu:121-159
 //
 // Deliberate differences from the reference, all in the direction of determinism:
 //   * strict Jacobi: iteration k reads only iteration k-1's dx and q (double buffers); the
@@ -88,16 +86,6 @@ __global__ void __launch_bounds__(256) k_end(Dev<R> d, int fb, int copyQ, int ka
     if (copyQ) d.q[0][i] = d.q[1][i];
 }
 
-template <typename R>
-__global__ void __launch_bounds__(128) k_step_limit(Dev<R> d) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= d.n) return;
-    const uint32_t flags = d.vp[k].flags;
-    R m = yinf<R>();
-    if (flags & F_HAS_NEXT) m = segment_step_limit(d, k, scene_params(d, flags), d.numCols[k]);
-    d.stepLim[k] = m;
-}
-
 // ---------------------------------------------------------------------------------------
 // IPC log barrier E(d) = -kCollision (d-1)^2 ln d on the normalised gap d, clamped to 1e-3:
 // returns dH = E''(d) / b^2 and the force magnitude ff (cosserat.cu:114-125).  Below d=1e-2
@@ -158,12 +146,26 @@ __device__ __forceinline__ void contact_term(V3<R> p0, V3<R> p1, V3<R> dx0, V3<R
 
 // ---------------------------------------------------------------------------------------
 // One block-Jacobi iteration: position solve (cosseratItr) then orientation update
-// (quaternionLambdaItr), strict Jacobi.  Block b handles vertices k = b*(B-2)-1+t,
-// t in [0,B): it writes vertices t in [1, B-2] and recomputes the halo t=0 and t=B-1.
-template <typename R, int B>
-__global__ void __launch_bounds__(B) k_iter(Dev<R> d, int src) {
+// (quaternionLambdaItr), strict Jacobi.  A block has B vertex slots of T lanes each
+// (NT = B*T threads): slot t handles vertex/segment k = b*(B-2)-1+t, writes it when
+// t in [1, B-2] and only recomputes the halo slots t=0 and t=B-1.  The T lanes of a slot
+// split the segment's contact loop (contacts s, s+T, ...) and combine their partial sums
+// with an xor-shuffle butterfly, so every lane of the slot holds the identical total; the
+// vertex solve and the orientation update are then evaluated by all T lanes and stored by
+// lane 0.
+template <typename R, int T>
+__device__ __forceinline__ R slot_sum(R v) {
+#pragma unroll
+    for (int o = 1; o < T; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <typename R, int NT, int T, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_iter(Dev<R> d, int src) {
+    constexpr int B = NT / T;
     constexpr int CORE = B - 2;
-    const int t = threadIdx.x;
+    const int t = threadIdx.x / T;
+    const int lane = threadIdx.x % T;
     const int k = blockIdx.x * CORE - 1 + t;
     const int n = d.n;
     const bool valid = (k >= 0) && (k < n);
@@ -198,40 +200,44 @@ __global__ void __launch_bounds__(B) k_iter(Dev<R> d, int src) {
         dx = xyz(DX[k]);
         q0 = qof(QO[k]);
         const R D = sp.D;
-        if (invMass != R(0)) {
-            // Inertia: H = m/h^2, f = m/h^2 (y - dx), y = h v + h^2 g (iteration.cu:26, cosserat.cu:40-45)
-            const V4<R> v = d.vel[k];
-            const R hh = sp.hh;
-            const V3<R> y(sp.h * v.x + hh * sp.gx, sp.h * v.y + hh * sp.gy, sp.h * v.z + hh * sp.gz);
-            Ha.diag(R(1) / (invMass * hh));
-            fa = (R(1) / (hh * invMass)) * (y - dx);
-        }
-        if (vp.cid >= 0) {
-            // Glue spring to the connected vertex (cosserat.cu:46-53)
-            const R stiff = R(40);
-            const V3<R> pc = xyz(d.pos[vp.cid]);
-            const V3<R> dc = xyz(DX[vp.cid]);
-            fa -= stiff * ((p0 - pc) + (dx - dc) + D * dx);
-            Ha.add_diag(stiff * (R(1) + D));
+        if (lane == 0) {
+            if (invMass != R(0)) {
+                // Inertia: H = m/h^2, f = m/h^2 (y - dx), y = h v + h^2 g (iteration.cu:26, cosserat.cu:40-45)
+                const V4<R> v = d.vel[k];
+                const R hh = sp.hh;
+                const V3<R> y(sp.h * v.x + hh * sp.gx, sp.h * v.y + hh * sp.gy, sp.h * v.z + hh * sp.gz);
+                Ha.diag(R(1) / (invMass * hh));
+                fa = (R(1) / (hh * invMass)) * (y - dx);
+            }
+            if (vp.cid >= 0) {
+                // Glue spring to the connected vertex (cosserat.cu:46-53)
+                const R stiff = R(40);
+                const V3<R> pc = xyz(d.pos[vp.cid]);
+                const V3<R> dc = xyz(DX[vp.cid]);
+                fa -= stiff * ((p0 - pc) + (dx - dc) + D * dx);
+                Ha.add_diag(stiff * (R(1) + D));
+            }
         }
         if (flags & F_HAS_NEXT) {
             p1 = xyz(d.pos[k + 1]);
             dx1 = xyz(DX[k + 1]);
             sl = d.stepLim[k];
-            // Stretch-shear coupling to the segment orientation (cosserat.cu:63-81)
-            const R invl = R(1) / lRest;
-            const V3<R> c = ((p1 - p0) + (dx1 - dx)) * invl - qrotate(q0, V3<R>(R(1), R(0), R(0)));
-            const R ks = kStretch * invl;
-            R dd = ks * invl;
-            fa += ks * c - (D * dd) * dx;
-            fb += -ks * c - (D * dd) * dx1;
-            dd *= R(1) + D;
-            Ha.add_diag(dd);
-            Hb.add_diag(dd);
-            // Barrier + friction over the contact list
+            if (lane == 0) {
+                // Stretch-shear coupling to the segment orientation (cosserat.cu:63-81)
+                const R invl = R(1) / lRest;
+                const V3<R> c = ((p1 - p0) + (dx1 - dx)) * invl - qrotate(q0, V3<R>(R(1), R(0), R(0)));
+                const R ks = kStretch * invl;
+                R dd = ks * invl;
+                fa += ks * c - (D * dd) * dx;
+                fb += -ks * c - (D * dd) * dx1;
+                dd *= R(1) + D;
+                Ha.add_diag(dd);
+                Hb.add_diag(dd);
+            }
+            // Barrier + friction over this lane's share of the contact list
             const int nc = d.numCols[k];
             const int* __restrict__ cl = d.cols + k;
-            for (int c2 = 0; c2 < nc; c2++) {
+            for (int c2 = lane; c2 < nc; c2 += T) {
                 const int j = __ldg(cl + (size_t)n * c2);
                 const V3<R> b0 = xyz(d.pos[j]);
                 const V3<R> b1 = xyz(d.pos[j + 1]);
@@ -241,10 +247,21 @@ __global__ void __launch_bounds__(B) k_iter(Dev<R> d, int src) {
             }
         }
     }
-    sFb[0][t] = fb.x; sFb[1][t] = fb.y; sFb[2][t] = fb.z;
+    if (T > 1) {
+        fa.x = slot_sum<R, T>(fa.x); fa.y = slot_sum<R, T>(fa.y); fa.z = slot_sum<R, T>(fa.z);
+        fb.x = slot_sum<R, T>(fb.x); fb.y = slot_sum<R, T>(fb.y); fb.z = slot_sum<R, T>(fb.z);
 #pragma unroll
-    for (int e = 0; e < 6; e++) sHb[e][t] = Hb.d[e];
-    sSL[t] = sl;
+        for (int e = 0; e < 6; e++) {
+            Ha.d[e] = slot_sum<R, T>(Ha.d[e]);
+            Hb.d[e] = slot_sum<R, T>(Hb.d[e]);
+        }
+    }
+    if (lane == 0) {
+        sFb[0][t] = fb.x; sFb[1][t] = fb.y; sFb[2][t] = fb.z;
+#pragma unroll
+        for (int e = 0; e < 6; e++) sHb[e][t] = Hb.d[e];
+        sSL[t] = sl;
+    }
     __syncthreads();
 
     // Vertex solve: own segment + previous segment's endpoint share (cosserat.cu:175-205)
@@ -264,13 +281,13 @@ __global__ void __launch_bounds__(B) k_iter(Dev<R> d, int src) {
             if (l > sl && l > R(0)) dxn *= sl / l;
         }
     }
-    sDX[0][t] = dxn.x; sDX[1][t] = dxn.y; sDX[2][t] = dxn.z;
+    if (lane == 0) { sDX[0][t] = dxn.x; sDX[1][t] = dxn.y; sDX[2][t] = dxn.z; }
     const bool core = valid && t >= 1 && t <= CORE;
-    if (core) d.dx[src ^ 1][k] = v4(dxn, R(0));
+    if (core && lane == 0) d.dx[src ^ 1][k] = v4(dxn, R(0));
     __syncthreads();
 
     // Orientation update of segment k (cosserat.cu:209-253)
-    if (core) {
+    if (core && lane == 0) {
         Q<R> qn = q0;
         if (!(flags & F_FIX_ORI) && (flags & F_HAS_NEXT)) {
             const V3<R> dxb(sDX[0][t + 1], sDX[1][t + 1], sDX[2][t + 1]);
@@ -289,9 +306,14 @@ __global__ void __launch_bounds__(B) k_iter(Dev<R> d, int src) {
                 const R s = qdot(qmul(qinv(q0), qq), qr) > R(0) ? R(1) : R(-1);
                 b = qadd(b, qscale(s, qmul(qq, qinv(qr))));
             }
-            const R lambda = len(v) + qlen(b);
-            const Q<R> vb1 = qmul(qmul(qmk(v, R(0)), b), qmk(R(1), R(0), R(0), R(0)));
-            qn = qnormalize(qadd(vb1, qscale(lambda, b)));
+            // A single-segment yarn has no bending neighbours (b = 0): the closed form is
+            // 0/0 there (the reference produces NaN); keep the orientation instead.
+            const R bl = qlen(b);
+            if (bl > R(0)) {
+                const R lambda = len(v) + bl;
+                const Q<R> vb1 = qmul(qmul(qmk(v, R(0)), b), qmk(R(1), R(0), R(0), R(0)));
+                qn = qnormalize(qadd(vb1, qscale(lambda, b)));
+            }
         }
         d.q[src ^ 1][k] = v4of(qn);
     }
@@ -310,34 +332,29 @@ void launch_end(const Dev<R>& d, int finalBuf, bool copyQ, bool kahan, cudaStrea
     k_end<R><<<(d.n + 255) / 256, 256, 0, s>>>(d, finalBuf, copyQ ? 1 : 0, kahan ? 1 : 0);
 }
 
+// Newton iteration launch shapes: NT threads per block, T lanes per vertex.
 template <typename R>
-void launch_step_limit(const Dev<R>& d, cudaStream_t s) {
+void launch_iter(const Dev<R>& d, int srcBuf, int threads, int lanes, cudaStream_t s) {
     if (d.n <= 0) return;
-    k_step_limit<R><<<(d.n + 127) / 128, 128, 0, s>>>(d);
-}
-
-template <typename R>
-void launch_iter(const Dev<R>& d, int srcBuf, int block, cudaStream_t s) {
-    if (d.n <= 0) return;
-    // FP64 at 512 threads would exceed the 48 KB static shared-memory limit: use 256.
-    if (sizeof(R) == 8 && block == 512) block = 256;
-    switch (block) {
-        case 64: k_iter<R, 64><<<(d.n + 61) / 62, 64, 0, s>>>(d, srcBuf); break;
-        case 128: k_iter<R, 128><<<(d.n + 125) / 126, 128, 0, s>>>(d, srcBuf); break;
-        case 512:
-            if constexpr (sizeof(R) == 4) k_iter<R, 512><<<(d.n + 509) / 510, 512, 0, s>>>(d, srcBuf);
-            break;
-        default: k_iter<R, 256><<<(d.n + 253) / 254, 256, 0, s>>>(d, srcBuf); break;
+#define YB_ITER(NT, T, MINB) \
+    k_iter<R, NT, T, MINB><<<(d.n + (NT / T) - 3) / ((NT / T) - 2), NT, 0, s>>>(d, srcBuf)
+    if (lanes == 2) {
+        YB_ITER(256, 2, 3);
+    } else if (lanes == 4) {
+        if (threads == 512) YB_ITER(512, 4, 2); else YB_ITER(256, 4, 3);
+    } else if (lanes == 8) {
+        if (threads == 512) YB_ITER(512, 8, 2); else YB_ITER(256, 8, 3);
+    } else {
+        if (threads == 128) YB_ITER(128, 1, 6); else YB_ITER(256, 1, 3);
     }
+#undef YB_ITER
 }
 
 template void launch_init<float>(const Dev<float>&, cudaStream_t);
 template void launch_init<double>(const Dev<double>&, cudaStream_t);
 template void launch_end<float>(const Dev<float>&, int, bool, bool, cudaStream_t);
 template void launch_end<double>(const Dev<double>&, int, bool, bool, cudaStream_t);
-template void launch_step_limit<float>(const Dev<float>&, cudaStream_t);
-template void launch_step_limit<double>(const Dev<double>&, cudaStream_t);
-template void launch_iter<float>(const Dev<float>&, int, int, cudaStream_t);
-template void launch_iter<double>(const Dev<double>&, int, int, cudaStream_t);
+template void launch_iter<float>(const Dev<float>&, int, int, int, cudaStream_t);
+template void launch_iter<double>(const Dev<double>&, int, int, int, cudaStream_t);
 
 }  // namespace yb

@@ -50,6 +50,7 @@ struct EngineBase {
     virtual uint64_t debug_phases(int mask, int& buf) = 0;
     virtual int64_t penetrations() = 0;
     virtual yb_status profile_substep(bool detect, bool rebuild, double* ms, uint64_t* launches) = 0;
+    virtual yb_status time_iter(int threads, int lanes, int reps, float* ms) = 0;
 };
 
 }  // namespace
@@ -71,7 +72,8 @@ struct yb_sim {
     float lastBVHRebuild = INFINITY;
     uint64_t stepCounter = 0;
     int lastErrorCode = 0, lastWarningCode = 0;
-    int iterBlock = 256;
+    int iterThreads = 256;
+    int iterLanes = 4;
     int useGraphs = 1;
     uint64_t launches = 0;
     cudaStream_t stream = nullptr;     // active stream (own or the caller's)
@@ -283,7 +285,7 @@ struct Engine : EngineBase {
     int* errHost = nullptr;
     cudaGraphExec_t graphs[GRAPH_TYPES] = {nullptr, nullptr, nullptr};
     uint64_t graphLaunches[GRAPH_TYPES] = {0, 0, 0};
-    int graphItr = -1, graphBlock = -1, graphNseg = -1;
+    int graphItr = -1, graphThreads = -1, graphLanes = -1, graphNseg = -1;
     int keyBits = 30;
     int64_t penTotal = 0;
 
@@ -447,13 +449,13 @@ struct Engine : EngineBase {
                 launch_bvh_refit(d, st);
                 k += d.nseg > 1 ? 1 : 0;
             }
-            launch_traverse(d, st); k++;
+            launch_traverse(d, st); k += 2;
         } else {
-            launch_step_limit(d, st); k++;
+            launch_lists_step_limit(d, st); k++;
         }
         const int I = num_itr();
         for (int it = 0; it < I; it++) {
-            launch_iter(d, it & 1, S->iterBlock, st);
+            launch_iter(d, it & 1, S->iterThreads, S->iterLanes, st);
             k++;
         }
         launch_end(d, I & 1, (I & 1) != 0, sizeof(R) == 4, st); k++;
@@ -465,7 +467,7 @@ struct Engine : EngineBase {
             if (g) cudaGraphExecDestroy(g);
             g = nullptr;
         }
-        graphItr = graphBlock = graphNseg = -1;
+        graphItr = graphThreads = graphLanes = graphNseg = -1;
     }
 
     yb_status run_substep(int type) override {
@@ -475,10 +477,12 @@ struct Engine : EngineBase {
             YB_CUDA(cudaGetLastError());
             return YB_OK;
         }
-        if (graphItr != num_itr() || graphBlock != S->iterBlock || graphNseg != d.nseg) {
+        if (graphItr != num_itr() || graphThreads != S->iterThreads || graphLanes != S->iterLanes ||
+            graphNseg != d.nseg) {
             invalidate_graphs();
             graphItr = num_itr();
-            graphBlock = S->iterBlock;
+            graphThreads = S->iterThreads;
+            graphLanes = S->iterLanes;
             graphNseg = d.nseg;
         }
         if (!graphs[type]) {
@@ -619,13 +623,13 @@ struct Engine : EngineBase {
                 launches[2] += d.nseg > 1 ? 1 : 0;
             }
             mark(3);
-            launch_traverse(d, st); launches[3]++;
+            launch_traverse(d, st); launches[3] += 2;
         } else {
             mark(4);
-            launch_step_limit(d, st); launches[4]++;
+            launch_lists_step_limit(d, st); launches[4]++;
         }
         mark(5);
-        for (int it = 0; it < I; it++) launch_iter(d, it & 1, S->iterBlock, st);
+        for (int it = 0; it < I; it++) launch_iter(d, it & 1, S->iterThreads, S->iterLanes, st);
         launches[5] += I;
         mark(6);
         launch_end(d, I & 1, (I & 1) != 0, sizeof(R) == 4, st); launches[6]++;
@@ -642,6 +646,29 @@ struct Engine : EngineBase {
         return cuda_status(e);
     }
 
+    // Average device time of one Newton iteration launch of the given shape on the current
+    // state.  Reads dx[0]/q[0] and writes only dx[1]/q[1], which hold nothing between
+    // substeps, so the simulation state is unchanged.
+    yb_status time_iter(int threads, int lanes, int reps, float* ms) override {
+        cudaStream_t st = S->stream;
+        cudaEvent_t e0, e1;
+        YB_CUDA(cudaEventCreate(&e0));
+        YB_CUDA(cudaEventCreate(&e1));
+        launch_iter(d, 0, threads, lanes, st);
+        cudaEventRecord(e0, st);
+        for (int r = 0; r < reps; r++) launch_iter(d, 0, threads, lanes, st);
+        cudaEventRecord(e1, st);
+        S->launches += reps + 1;
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        float t = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        *ms = t / reps;
+        return cuda_status(e);
+    }
+
     uint64_t debug_phases(int mask, int& buf) override {
         cudaStream_t st = S->stream;
         uint64_t k = 0;
@@ -650,10 +677,10 @@ struct Engine : EngineBase {
             if (mask & 2) launch_bvh_rebuild(d, st, sortScratch, sortBytes, keyBits);
             else launch_bvh_refit(d, st);
             launch_traverse(d, st);
-            k += 2;
+            k += 3;
         }
-        if (mask & 8) { launch_step_limit(d, st); k++; }
-        if (mask & 16) { launch_iter(d, buf, S->iterBlock, st); buf ^= 1; k++; }
+        if (mask & 8) { launch_lists_step_limit(d, st); k++; }
+        if (mask & 16) { launch_iter(d, buf, S->iterThreads, S->iterLanes, st); buf ^= 1; k++; }
         if (mask & 32) { launch_end(d, buf, buf != 0, sizeof(R) == 4, st); buf = 0; k++; }
         return k;
     }
@@ -977,20 +1004,50 @@ const char* yb_status_string(yb_status s) {
     return "unknown status";
 }
 
-yb_status yb_set_tuning(yb_sim* S, int32_t iterBlock, int32_t useGraphs) {
-    if (!S) return YB_ERR_INVALID_ARGUMENT;
-    if (iterBlock != 64 && iterBlock != 128 && iterBlock != 256 && iterBlock != 512) return YB_ERR_INVALID_ARGUMENT;
-    S->iterBlock = iterBlock;
+static bool valid_shape(int threads, int lanes) {
+    return (lanes == 1 && (threads == 128 || threads == 256)) || (lanes == 2 && threads == 256) ||
+           ((lanes == 4 || lanes == 8) && (threads == 256 || threads == 512));
+}
+
+yb_status yb_set_tuning(yb_sim* S, int32_t iterThreads, int32_t lanesPerVertex, int32_t useGraphs) {
+    if (!S || !valid_shape(iterThreads, lanesPerVertex)) return YB_ERR_INVALID_ARGUMENT;
+    S->iterThreads = iterThreads;
+    S->iterLanes = lanesPerVertex;
     S->useGraphs = useGraphs ? 1 : 0;
     if (S->eng) S->eng->invalidate_graphs();
     return YB_OK;
 }
 
-yb_status yb_get_tuning(yb_sim* S, int32_t* iterBlock, int32_t* useGraphs) {
+yb_status yb_get_tuning(yb_sim* S, int32_t* iterThreads, int32_t* lanesPerVertex, int32_t* useGraphs) {
     if (!S) return YB_ERR_INVALID_ARGUMENT;
-    if (iterBlock) *iterBlock = S->iterBlock;
+    if (iterThreads) *iterThreads = S->iterThreads;
+    if (lanesPerVertex) *lanesPerVertex = S->iterLanes;
     if (useGraphs) *useGraphs = S->useGraphs;
     return YB_OK;
+}
+
+yb_status yb_autotune(yb_sim* S, int32_t* bestThreads, int32_t* bestLanes, float* bestMs) {
+    if (!S) return YB_ERR_INVALID_ARGUMENT;
+    if (!S->configured) return YB_ERR_NOT_CONFIGURED;
+    static const int shapes[][2] = {{256, 1}, {128, 1}, {256, 2}, {256, 4}, {512, 4}, {256, 8}, {512, 8}};
+    float best = INFINITY;
+    int bt = S->iterThreads, bl = S->iterLanes;
+    S->eng->write_params();
+    for (const auto& sh : shapes) {
+        float ms = 0.f;
+        const yb_status st = S->eng->time_iter(sh[0], sh[1], 5, &ms);
+        if (st != YB_OK) return st;
+        if (ms < best) {
+            best = ms;
+            bt = sh[0];
+            bl = sh[1];
+        }
+    }
+    const yb_status st = yb_set_tuning(S, bt, bl, S->useGraphs);
+    if (bestThreads) *bestThreads = bt;
+    if (bestLanes) *bestLanes = bl;
+    if (bestMs) *bestMs = best;
+    return st;
 }
 
 yb_status yb_set_stream(yb_sim* S, void* stream) {

@@ -206,8 +206,20 @@ class Sim:
         return np.ctypeslib.as_array(p, shape=(c.value,)).copy()
 
     # ---- additions -------------------------------------------------------------------
-    def set_tuning(self, iterBlock=256, useGraphs=True):
-        check(self._lib.yb_set_tuning(self._h, int(iterBlock), 1 if useGraphs else 0), "tuning")
+    def set_tuning(self, iterThreads=256, lanesPerVertex=4, useGraphs=True):
+        check(self._lib.yb_set_tuning(self._h, int(iterThreads), int(lanesPerVertex), 1 if useGraphs else 0),
+              "tuning")
+
+    def get_tuning(self):
+        t, l, g = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        check(self._lib.yb_get_tuning(self._h, ctypes.byref(t), ctypes.byref(l), ctypes.byref(g)))
+        return t.value, l.value, bool(g.value)
+
+    def autotune(self):
+        """Times every Newton-kernel shape on the current state and keeps the fastest."""
+        t, l, ms = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_float()
+        check(self._lib.yb_autotune(self._h, ctypes.byref(t), ctypes.byref(l), ctypes.byref(ms)), "autotune")
+        return t.value, l.value, ms.value
 
     def set_stream(self, stream_handle):
         """Launch on a caller's cudaStream_t (int handle, e.g. torch's stream.cuda_stream); 0 = own."""
