@@ -232,7 +232,7 @@ def run_ours(args):
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    from yarnball_b200 import scenes
+    from yarnball_b200 import scenes, sharding
 
     spec = scenes.batched_spec(SEED + 1000 * rank, 512, args.cap)
     n, cfg = workload_desc(spec)
@@ -268,15 +268,7 @@ def run_ours(args):
     ck = clocks.stop()
     launches = sim.launch_count() - l0
     ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms, float(n)], device="cuda", dtype=torch.float64)
-    if dist:
-        tmax = t.clone()
-        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
-        tsum = t.clone()
-        dist.all_reduce(tsum[1:], op=dist.ReduceOp.SUM)
-        ms_max, n_all = float(tmax[0]), float(tsum[1])
-    else:
-        ms_max, n_all = ms, float(n)
+    ms_max, n_all = sharding.reduce_timing(ms, n, device="cuda")
     value = n_all * SUBSTEPS * args.steps / (ms_max / 1e3)
 
     # Per-kernel device times of one more frame (events around each kernel class).
@@ -322,11 +314,7 @@ def run_ours(args):
     f1.record(stream)
     torch.cuda.synchronize()
     wall = time.perf_counter() - w0
-    ems = f0.elapsed_time(f1)
-    if dist:
-        tt = torch.tensor([ems], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ems = float(tt[0])
+    ems, _ = sharding.reduce_timing(f0.elapsed_time(f1), n, device="cuda")
     e2e = {"value": n_all * SUBSTEPS * e2e_steps / (ems / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h, "steps": e2e_steps, "wall_s": wall,
            "api": "yb_upload + yb_advance + yb_download (pinned host arrays)"}

@@ -1,0 +1,68 @@
+"""Multi-rank logic on CPU: two gloo ranks partition the batched workload's scenes and reduce
+timings the way bench.py does on GPUs (no GPU involved)."""
+import os
+import socket
+
+import numpy as np
+import torch.multiprocessing as mp
+
+from yarnball_b200 import scenes, sharding
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _worker(rank, world, port, sizes, out):
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    parts = sharding.partition_scenes(sizes, world)
+    mine = parts[rank]
+    verts = int(sum(sizes[i] for i in mine))
+    ms, total = sharding.reduce_timing(10.0 + rank, verts)
+    stats = sharding.reduce_stats([1.0, float(verts)])
+    out[rank] = (mine, ms, total, stats.tolist())
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_partition_is_complete_disjoint_and_balanced():
+    yarns, lens, _ = scenes.batched_spec()
+    sizes = [int(l.sum()) for l in lens]
+    for world in (1, 2, 4, 8):
+        parts = sharding.partition_scenes(sizes, world)
+        flat = sorted(i for p in parts for i in p)
+        assert flat == list(range(len(sizes)))
+        loads = [sum(sizes[i] for i in p) for p in parts]
+        # greedy longest-first: the spread is at most the largest scene
+        assert max(loads) - min(loads) <= max(sizes)
+    assert sharding.partition_scenes(sizes, 3) == sharding.partition_scenes(sizes, 3)
+
+
+def test_two_gloo_ranks_agree_on_partition_and_reduce():
+    yarns, lens, _ = scenes.batched_spec(num_scenes=40, cap=1_000_000)
+    sizes = [int(l.sum()) for l in lens]
+    world = 2
+    port = _free_port()
+    with mp.Manager() as mgr:
+        out = mgr.dict()
+        mp.spawn(_worker, args=(world, port, sizes, out), nprocs=world, join=True)
+        res = dict(out)
+    parts = sharding.partition_scenes(sizes, world)
+    for r in range(world):
+        mine, ms, total, stats = res[r]
+        assert mine == parts[r]
+        assert ms == 11.0  # max over ranks
+        assert total == float(sum(sizes))
+        assert stats[0] == 2.0 and stats[1] == float(sum(sizes))
+    assert sorted(res[0][0] + res[1][0]) == list(range(len(sizes)))
+    np.testing.assert_equal(len(set(res[0][0]) & set(res[1][0])), 0)
