@@ -130,6 +130,23 @@ def test_pile_small_substep_vs_fp64():
     assert qerr <= 1e-5, qerr
 
 
+def test_dense_pile_substep_vs_fp64():
+    """Contact-heavy: 96 yarns x 64 vertices in a 3 cm cube (segments with more contacts than
+    the staged ones exercise both contact paths of the Newton kernel)."""
+    sim = scenes.build_pile(seed=9, yarns=96, verts=64, cube=0.03)
+    orc = oracle.from_sim(sim, mode=oracle.FP64)
+    sim.advance(1e-3)
+    orc.advance(1e-3, 1e-3)
+    nc, _, _ = sim.debug_contacts()
+    assert nc.max() > 8 and nc.mean() > 2
+    pos, _, q = sim.read_state_f64()
+    ref = orc.state()
+    perr = np.abs(pos - ref["pos"]).max()
+    assert perr <= 1e-5 * SEG, perr
+    qerr = quat_angle(q[seg_rows(sim)], ref["q"][seg_rows(sim)]).max()
+    assert qerr <= 1e-5, qerr
+
+
 def test_batched_equals_alone():
     spec = scenes.batched_spec(seed=5, num_scenes=5, cap=200000, max_yarns=12, min_len=32, max_len=400)
     assert len(spec[0]) == 5

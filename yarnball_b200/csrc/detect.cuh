@@ -25,8 +25,9 @@ __device__ __forceinline__ Box<R> segment_box(const Dev<R>& d, int k, const Scen
     const V4<R> p1 = d.pos[k + 1];
     R pad = sp.sdr;
     if (sp.useVelRadius) {
-        const R l0 = xlen2(xyz(d.dx[0][k]));
-        const R l1 = xlen2(xyz(d.dx[0][k + 1]));
+        const D2<R> dk = d.dx[0][k];
+        const R l0 = xlen2(xyz(dk.a));
+        const R l1 = xlen2(xyz(dk.b));
         pad = E::add(pad, E::sqrt(ymax(l0, l1)));
     }
     Box<R> b;
@@ -63,27 +64,38 @@ __device__ __forceinline__ bool pair_keep(const Dev<R>& d, int x, int y, const S
     const R d2 = xlen2(nrm);
     R r = E::mul(R(2), sp.sdr);
     if (sp.useVelRadius) {
-        r = E::add(r, E::sqrt(ymax(xlen2(xyz(d.dx[0][x])), xlen2(xyz(d.dx[0][x + 1])))));
-        r = E::add(r, E::sqrt(ymax(xlen2(xyz(d.dx[0][y])), xlen2(xyz(d.dx[0][y + 1])))));
+        const D2<R> dxx = d.dx[0][x], dxy = d.dx[0][y];
+        r = E::add(r, E::sqrt(ymax(xlen2(xyz(dxx.a)), xlen2(xyz(dxx.b)))));
+        r = E::add(r, E::sqrt(ymax(xlen2(xyz(dxy.a)), xlen2(xyz(dxy.b)))));
     }
     return d2 < E::mul(r, r);
 }
 
 // Step-size limit of segment k over its nc listed contacts.  Also counts contacts whose
-// centre-line distance is at or below 2 * radius (interpenetration), each unordered pair once.
+// centre-line distance is at or below 2 * radius (interpenetration), each unordered pair once,
+// and stages the partner endpoints relative to p0 for the first RELCAP contacts (read by
+// every Newton iteration of the substep).
 template <typename R>
 __device__ __forceinline__ R segment_step_limit(const Dev<R>& d, int k, const SceneParams<R>& sp, int nc) {
     typedef Ex<R> E;
     const V3<R> a0 = xyz(d.pos[k]);
     const V3<R> a1 = xsub(xyz(d.pos[k + 1]), a0);
     R m = sp.stepBase;
-    if (sp.useVelRadius) m = E::add(m, E::sqrt(xlen2(xyz(d.dx[0][k]))));
+    if (sp.useVelRadius) m = E::add(m, E::sqrt(xlen2(xyz(d.dx[0][k].a))));
     const R safe = E::mul(E::sub(R(1), R(0.1f)), R(0.5f));
     int pen = 0;
     for (int c = 0; c < nc; c++) {
         const int o = d.cols[k + (size_t)d.n * c];
         const V3<R> b0 = xsub(xyz(d.pos[o]), a0);
         const V3<R> b1 = xsub(xyz(d.pos[o + 1]), a0);
+        if (c < RELCAP) {
+            const size_t at = k + (size_t)d.n * c;
+            d.relA[at] = v4(b0, b1.x);
+            R2<R> rb;
+            rb.x = b1.y;
+            rb.y = b1.z;
+            d.relB[at] = rb;
+        }
         const UVT<R> uv = closest_uv_exact(a1, b0, b1);
         const V3<R> nrm = xsub(xscale(uv.u, a1), xmix(b0, b1, uv.v));
         const R l = E::sqrt(xlen2(nrm));

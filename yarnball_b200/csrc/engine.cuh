@@ -6,13 +6,14 @@
 //   vel      V4<R>  xyz = velocity (kept intact during the iterations; y = h v + h^2 g is
 //                   formed on the fly instead of overwriting vel as YarnBall.cu does)
 //   lastVel  V4<R>  velocity of the previous substep (acceleration-aware initial guess)
-//   dx[2]    V4<R>  Newton iterate (double buffered: strict Jacobi)
+//   dx[2]    D2<R>  Newton iterate of k and k+1 (double buffered: strict Jacobi)
 //   q[2]     V4<R>  segment orientation rotor (double buffered)
 //   qRest    V4<R>  rest Darboux rotor; its magnitude is the bending stiffness
 //   vp       VP<R>  {lRest, kStretch, connectionIndex, flags | scene << 8}
 //   stepLim  R      per-segment displacement limit (collision.cu:121-159)
 //   numCols  int    contacts of each segment
 //   cols     int    contact partner ids, column major: cols[seg + n * k], k < MAX_COLS
+//   relA/B   V4,R2  partner endpoints relative to p0 for the first RELCAP contacts
 // Segments are the vertices with hasNext; segs[] lists them and is the leaf set of the BVH.
 #pragma once
 #include "ybmath.cuh"
@@ -41,6 +42,21 @@ enum {
     EW_COUNT = 8
 };
 enum { IE_BVH_STACK = 1, IE_SORT_WAIT = 2, IE_GRID_WAIT = 4, IE_REFIT = 8 };
+
+// The Newton iterate of vertex k stored together with that of vertex k+1, so that a segment's
+// two endpoints come from one 32-byte sector (one gather per contact partner).
+template <typename R>
+struct alignas(sizeof(R) * 8) D2 {
+    V4<R> a;  // dx[k]
+    V4<R> b;  // dx[k+1] (zero for the last vertex)
+};
+
+template <typename R>
+struct alignas(sizeof(R) * 2) R2 {
+    R x, y;
+};
+
+constexpr int RELCAP = 8;  // contacts per segment with staged relative partner positions
 
 template <typename R>
 struct VP {
@@ -81,13 +97,15 @@ struct Dev {
     V4<R>* posC;
     V4<R>* vel;
     V4<R>* lastVel;
-    V4<R>* dx[2];
+    D2<R>* dx[2];     // iterate pairs (dx[k], dx[k+1]), double buffered
     V4<R>* q[2];
     V4<R>* qRest;
     VP<R>* vp;
     R* stepLim;
     int* numCols;
     int* cols;
+    V4<R>* relA;      // staged per substep for contacts c < RELCAP, column major [seg + n*c]:
+    R2<R>* relB;      //   relA = (b0 - p0, (b1 - p0).x), relB = (b1 - p0).yz
     int* segs;        // segment -> vertex index, ascending (scene-contiguous)
     const SceneParams<R>* sp;
     int* err;         // EW_COUNT ints

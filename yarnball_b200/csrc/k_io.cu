@@ -77,7 +77,7 @@ __global__ void k_state_f64(Dev<R> d, int buf, double* pos, double* vel, double*
     if (pos) { const V4<R> p = d.pos[i]; pos[3 * i] = p.x; pos[3 * i + 1] = p.y; pos[3 * i + 2] = p.z; }
     if (vel) { const V4<R> v = d.vel[i]; vel[3 * i] = v.x; vel[3 * i + 1] = v.y; vel[3 * i + 2] = v.z; }
     if (q) { const V4<R> a = d.q[buf][i]; q[4 * i] = a.x; q[4 * i + 1] = a.y; q[4 * i + 2] = a.z; q[4 * i + 3] = a.w; }
-    if (dx) { const V4<R> a = d.dx[buf][i]; dx[4 * i] = a.x; dx[4 * i + 1] = a.y; dx[4 * i + 2] = a.z; dx[4 * i + 3] = a.w; }
+    if (dx) { const V4<R> a = d.dx[buf][i].a; dx[4 * i] = a.x; dx[4 * i + 1] = a.y; dx[4 * i + 2] = a.z; dx[4 * i + 3] = a.w; }
 }
 
 // Root box of each scene's subtree (refit must have run).

@@ -24,35 +24,44 @@ __device__ __forceinline__ const SceneParams<R>& scene_params(const Dev<R>& d, u
 
 // ---------------------------------------------------------------------------------------
 // Predictor (iteration.cu:7-41).  Every operation separately rounded: dx0 feeds the
-// bit-exact collision filter through the velocity radius.
+// bit-exact collision filter through the velocity radius.  Reads only; the reference's
+// `lastVels = vel` store happens in k_end instead, so that thread i can also predict vertex
+// i+1 for the iterate pair without racing with thread i+1.
 template <typename R>
-__global__ void __launch_bounds__(256) k_init(Dev<R> d) {
+__device__ __forceinline__ V3<R> predict(const Dev<R>& d, int i) {
     typedef Ex<R> E;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= d.n) return;
-    const uint32_t flags = d.vp[i].flags;
-    const SceneParams<R>& sp = scene_params(d, flags);
+    const SceneParams<R>& sp = d.sp[scene_of(d.vp[i].flags)];
     const V4<R> vel4 = d.vel[i];
     const V4<R> lv4 = d.lastVel[i];
-    d.lastVel[i] = vel4;
     const R h = sp.h;
-    V3<R> v = xyz(vel4);
+    const V3<R> v = xyz(vel4);
     V3<R> dx = xscale(h, v);
     if (d.pos[i].w != R(0)) {
         const R g2 = sp.g2;
         if (g2 > R(0)) {
             const V3<R> g(sp.gx, sp.gy, sp.gz);
-            V3<R> a(E::div(E::sub(v.x, lv4.x), sp.lastH), E::div(E::sub(v.y, lv4.y), sp.lastH),
-                    E::div(E::sub(v.z, lv4.z), sp.lastH));
-            R s = yclamp(E::div(xdot(a, g), g2), R(0), R(1));
+            const V3<R> a(E::div(E::sub(v.x, lv4.x), sp.lastH), E::div(E::sub(v.y, lv4.y), sp.lastH),
+                          E::div(E::sub(v.z, lv4.z), sp.lastH));
+            const R s = yclamp(E::div(xdot(a, g), g2), R(0), R(1));
             dx = xadd(dx, xscale(E::mul(E::mul(h, h), s), g));
         }
     }
-    d.dx[0][i] = v4(dx, R(0));
+    return dx;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_init(Dev<R> d) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.n) return;
+    D2<R> o;
+    o.a = v4(predict(d, i), R(0));
+    o.b = v4(i + 1 < d.n ? predict(d, i + 1) : V3<R>(R(0)), R(0));
+    d.dx[0][i] = o;
 }
 
 // ---------------------------------------------------------------------------------------
-// Advection (iteration.cu:48-61) with Kahan-compensated position accumulation (FP32 build).
+// Advection (iteration.cu:48-61) with Kahan-compensated position accumulation (FP32 build);
+// also stores the start-of-substep velocity as lastVel (iteration.cu:19-20).
 template <typename R>
 __global__ void __launch_bounds__(256) k_end(Dev<R> d, int fb, int copyQ, int kahan) {
     typedef Ex<R> E;
@@ -60,8 +69,9 @@ __global__ void __launch_bounds__(256) k_end(Dev<R> d, int fb, int copyQ, int ka
     if (i >= d.n) return;
     const uint32_t flags = d.vp[i].flags;
     const SceneParams<R>& sp = scene_params(d, flags);
-    const V4<R> dx = d.dx[fb][i];
+    const V4<R> dx = d.dx[fb][i].a;
     V4<R> p = d.pos[i];
+    d.lastVel[i] = d.vel[i];
     if (p.w != R(0)) {
         V4<R> v;
         v.x = dx.x * sp.invH * sp.dragFactor;
@@ -106,14 +116,15 @@ __device__ __forceinline__ void barrier_terms(R d, R kCol, R invb, R& dH, R& ff)
     }
 }
 
-// Contact of segment (p0,p1) with segment (b0,b1) on the current iterate (cosserat.cu:92-148).
-// Accumulates into the forces/Hessians of the segment's two endpoints.
+// Contact of segment (p0,p1) with segment (b0,b1) on the current iterate (cosserat.cu:92-148),
+// in coordinates relative to p0: e = p1 - p0, r0 = b0 - p0, r1 = b1 - p0 (the closest points
+// and the gap only depend on differences).  Accumulates into the forces/Hessians of the
+// segment's two endpoints.
 template <typename R>
-__device__ __forceinline__ void contact_term(V3<R> p0, V3<R> p1, V3<R> dx0, V3<R> dx1, V3<R> b0, V3<R> b1,
-                                             V3<R> db0, V3<R> db1, const SceneParams<R>& sp, V3<R>& fa,
-                                             H3<R>& Ha, V3<R>& fb, H3<R>& Hb) {
-    const UVT<R> uv = closest_uv((p1 - p0) + (dx1 - dx0), (b0 - p0) + (db0 - dx0), (b1 - p0) + (db1 - dx0));
-    const V3<R> dpos = mix(p0, p1, uv.u) - mix(b0, b1, uv.v);
+__device__ __forceinline__ void contact_term(V3<R> e, V3<R> dx0, V3<R> dx1, V3<R> r0, V3<R> r1, V3<R> db0, V3<R> db1,
+                                             const SceneParams<R>& sp, V3<R>& fa, H3<R>& Ha, V3<R>& fb, H3<R>& Hb) {
+    const UVT<R> uv = closest_uv(e + (dx1 - dx0), r0 + (db0 - dx0), r1 + (db1 - dx0));
+    const V3<R> dpos = uv.u * e - mix(r0, r1, uv.v);
     const V3<R> ddpos = mix(dx0, dx1, uv.u) - mix(db0, db1, uv.v);
     V3<R> nrm = dpos + ddpos;
     const R dist = len(nrm);
@@ -169,7 +180,7 @@ __global__ void __launch_bounds__(NT, MINB) k_iter(Dev<R> d, int src) {
     const int k = blockIdx.x * CORE - 1 + t;
     const int n = d.n;
     const bool valid = (k >= 0) && (k < n);
-    const V4<R>* __restrict__ DX = d.dx[src];
+    const D2<R>* __restrict__ DX = d.dx[src];
     const V4<R>* __restrict__ QO = d.q[src];
 
     __shared__ R sFb[3][B];
@@ -197,7 +208,9 @@ __global__ void __launch_bounds__(NT, MINB) k_iter(Dev<R> d, int src) {
         const V4<R> P = d.pos[k];
         p0 = xyz(P);
         invMass = P.w;
-        dx = xyz(DX[k]);
+        const D2<R> own = DX[k];
+        dx = xyz(own.a);
+        dx1 = xyz(own.b);
         q0 = qof(QO[k]);
         const R D = sp.D;
         if (lane == 0) {
@@ -213,14 +226,13 @@ __global__ void __launch_bounds__(NT, MINB) k_iter(Dev<R> d, int src) {
                 // Glue spring to the connected vertex (cosserat.cu:46-53)
                 const R stiff = R(40);
                 const V3<R> pc = xyz(d.pos[vp.cid]);
-                const V3<R> dc = xyz(DX[vp.cid]);
+                const V3<R> dc = xyz(DX[vp.cid].a);
                 fa -= stiff * ((p0 - pc) + (dx - dc) + D * dx);
                 Ha.add_diag(stiff * (R(1) + D));
             }
         }
         if (flags & F_HAS_NEXT) {
             p1 = xyz(d.pos[k + 1]);
-            dx1 = xyz(DX[k + 1]);
             sl = d.stepLim[k];
             if (lane == 0) {
                 // Stretch-shear coupling to the segment orientation (cosserat.cu:63-81)
@@ -234,16 +246,27 @@ __global__ void __launch_bounds__(NT, MINB) k_iter(Dev<R> d, int src) {
                 Ha.add_diag(dd);
                 Hb.add_diag(dd);
             }
-            // Barrier + friction over this lane's share of the contact list
+            // Barrier + friction over this lane's share of the contact list.  Partner
+            // positions relative to p0 are staged per substep for the first RELCAP contacts;
+            // the partner's iterate pair is one 32-byte gather.
             const int nc = d.numCols[k];
             const int* __restrict__ cl = d.cols + k;
+            const V3<R> e = p1 - p0;
             for (int c2 = lane; c2 < nc; c2 += T) {
+                const size_t at = k + (size_t)n * c2;
                 const int j = __ldg(cl + (size_t)n * c2);
-                const V3<R> b0 = xyz(d.pos[j]);
-                const V3<R> b1 = xyz(d.pos[j + 1]);
-                const V3<R> db0 = xyz(DX[j]);
-                const V3<R> db1 = xyz(DX[j + 1]);
-                contact_term(p0, p1, dx, dx1, b0, b1, db0, db1, sp, fa, Ha, fb, Hb);
+                V3<R> r0, r1;
+                if (c2 < RELCAP) {
+                    const V4<R> A = d.relA[at];
+                    const R2<R> Bq = d.relB[at];
+                    r0 = V3<R>(A.x, A.y, A.z);
+                    r1 = V3<R>(A.w, Bq.x, Bq.y);
+                } else {
+                    r0 = xyz(d.pos[j]) - p0;
+                    r1 = xyz(d.pos[j + 1]) - p0;
+                }
+                const D2<R> pd = DX[j];
+                contact_term(e, dx, dx1, r0, r1, xyz(pd.a), xyz(pd.b), sp, fa, Ha, fb, Hb);
             }
         }
     }
@@ -283,14 +306,17 @@ __global__ void __launch_bounds__(NT, MINB) k_iter(Dev<R> d, int src) {
     }
     if (lane == 0) { sDX[0][t] = dxn.x; sDX[1][t] = dxn.y; sDX[2][t] = dxn.z; }
     const bool core = valid && t >= 1 && t <= CORE;
-    if (core && lane == 0) d.dx[src ^ 1][k] = v4(dxn, R(0));
     __syncthreads();
 
-    // Orientation update of segment k (cosserat.cu:209-253)
+    // New iterate pair and orientation update of segment k (cosserat.cu:209-253)
     if (core && lane == 0) {
+        const V3<R> dxb(sDX[0][t + 1], sDX[1][t + 1], sDX[2][t + 1]);
+        D2<R> o;
+        o.a = v4(dxn, R(0));
+        o.b = v4(k + 1 < n ? dxb : V3<R>(R(0)), R(0));
+        d.dx[src ^ 1][k] = o;
         Q<R> qn = q0;
         if (!(flags & F_FIX_ORI) && (flags & F_HAS_NEXT)) {
-            const V3<R> dxb(sDX[0][t + 1], sDX[1][t + 1], sDX[2][t + 1]);
             V3<R> v = ((p1 - p0) + (dxb - dxn)) * (R(1) / lRest);
             v *= R(-2) * kStretch;
             Q<R> b = qmk(R(0), R(0), R(0), R(0));
@@ -345,7 +371,7 @@ void launch_iter(const Dev<R>& d, int srcBuf, int threads, int lanes, cudaStream
     } else if (lanes == 8) {
         if (threads == 512) YB_ITER(512, 8, 2); else YB_ITER(256, 8, 3);
     } else {
-        if (threads == 128) YB_ITER(128, 1, 6); else YB_ITER(256, 1, 3);
+        if (threads == 128) YB_ITER(128, 1, 6); else YB_ITER(256, 1, 2);
     }
 #undef YB_ITER
 }

@@ -311,8 +311,8 @@ struct Engine : EngineBase {
         want((void**)&d.posC, sizeof(V4<R>) * n);
         want((void**)&d.vel, sizeof(V4<R>) * n);
         want((void**)&d.lastVel, sizeof(V4<R>) * n);
-        want((void**)&d.dx[0], sizeof(V4<R>) * n);
-        want((void**)&d.dx[1], sizeof(V4<R>) * n);
+        want((void**)&d.dx[0], sizeof(D2<R>) * n);
+        want((void**)&d.dx[1], sizeof(D2<R>) * n);
         want((void**)&d.q[0], sizeof(V4<R>) * n);
         want((void**)&d.q[1], sizeof(V4<R>) * n);
         want((void**)&d.qRest, sizeof(V4<R>) * n);
@@ -320,6 +320,8 @@ struct Engine : EngineBase {
         want((void**)&d.stepLim, sizeof(R) * n);
         want((void**)&d.numCols, sizeof(int) * n);
         want((void**)&d.cols, sizeof(int) * n * MAX_COLS);
+        want((void**)&d.relA, sizeof(V4<R>) * n * RELCAP);
+        want((void**)&d.relB, sizeof(R2<R>) * n * RELCAP);
         want((void**)&d.segs, sizeof(int) * n);
         want((void**)&spDev, sizeof(SceneParams<R>) * ns);
         want((void**)&d.err, sizeof(int) * EW_COUNT);

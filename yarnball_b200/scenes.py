@@ -101,9 +101,9 @@ def fill_yarns(sim, pos, yarn_lengths, offset=0, pin_first=True, pin_last=False)
         v["invMass"][:] = im
 
 
-def build_pile(seed=1, yarns=1024, verts=256, precision="fp32", num_itr=None, meta=None):
+def build_pile(seed=1, yarns=1024, verts=256, precision="fp32", num_itr=None, meta=None, cube=CUBE):
     lens = np.full(yarns, verts, np.int32)
-    pos = random_walks(seed, lens)
+    pos = random_walks(seed, lens, cube=cube)
     sim = Sim(int(lens.sum()), precision=precision)
     fill_yarns(sim, pos, lens, pin_first=True)
     for k, val in dict(PILE_META, **(meta or {})).items():
