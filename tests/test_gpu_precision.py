@@ -1,0 +1,59 @@
+"""FP32 production build against the FP64 build of the same kernels, per workload, after one
+frame (34 substeps) from identical inputs.  Relative error = max position difference /
+max displacement over the frame (the north-star bound is 1e-4).  Orientation error is the
+largest angle between corresponding segment rotors."""
+import numpy as np
+import pytest
+
+from yarnball_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+FRAME = 1 / 30.0
+
+
+def _angle(q1, q2):
+    s = np.sign(np.sum(q1 * q2, axis=1, keepdims=True))
+    s[s == 0] = 1
+    return 2 * np.arctan2(np.linalg.norm(q1 - s * q2, axis=1), np.linalg.norm(q1 + s * q2, axis=1))
+
+
+def _frame_errors(build, frames=1, driver=None):
+    a, b = build("fp32"), build("fp64")
+    x0 = b.read_state_f64()[0]
+    if driver:
+        da, db = driver(a), driver(b)
+        for _ in range(frames):
+            da.frame(FRAME)
+            db.frame(FRAME)
+    else:
+        for _ in range(frames):
+            a.advance(FRAME)
+            b.advance(FRAME)
+    pa, _, qa = a.read_state_f64()
+    pb, _, qb = b.read_state_f64()
+    seg = (b.verts["flags"] & 2) != 0
+    rel = np.abs(pa - pb).max() / max(np.abs(pb - x0).max(), 1e-30)
+    ang = _angle(qa[seg], qb[seg]).max()
+    return rel, ang
+
+
+def test_readme_fp32_vs_fp64():
+    rel, ang = _frame_errors(lambda p: scenes.build_readme(precision=p))
+    assert rel <= 1e-4 and ang <= 1e-4, (rel, ang)
+
+
+def test_pile_fp32_vs_fp64():
+    rel, ang = _frame_errors(lambda p: scenes.build_pile(seed=1, precision=p))
+    assert rel <= 1e-4, (rel, ang)
+
+
+def test_twist_fp32_vs_fp64():
+    rel, ang = _frame_errors(lambda p: scenes.build_twist(precision=p), driver=scenes.TwistDriver)
+    assert rel <= 1e-4, (rel, ang)
+
+
+def test_batched_fp32_vs_fp64():
+    spec = scenes.batched_spec(seed=5, num_scenes=24, cap=600000)
+    rel, ang = _frame_errors(lambda p: scenes.build_batched(seed=5, spec=spec, precision=p)[0])
+    assert rel <= 1e-4, (rel, ang)

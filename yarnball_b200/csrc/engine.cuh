@@ -82,7 +82,7 @@ struct SceneParams {
 };
 
 template <typename R>
-struct BNode {                     // internal BVH node: boxes of both children + links
+struct alignas(16) BNode {         // internal BVH node: boxes of both children + links
     R lmin[3], lmax[3], rmin[3], rmax[3];
     int left, right;               // child code: >= 0 internal node, < 0 leaf -(seg + 1)
     int parent, pad;

@@ -221,30 +221,45 @@ __device__ __forceinline__ void list_append(const Dev<R>& d, int x, int y) {
     if (pos < MAX_COLS) d.cols[x + (size_t)d.n * pos] = y;
 }
 
-// Broadphase + narrow phase.  Each lane walks its own segment's scene subtree; a leaf whose
-// box overlaps and whose segment index is larger than the query's becomes a candidate pair
-// in a per-warp queue.  Whenever 32 candidates are queued, the whole warp runs the
-// separately rounded narrow-phase test on them, one pair per lane, so the expensive test
-// never runs with idle lanes; kept pairs are appended to both segments' lists.
+// Broadphase + narrow phase, one warp per 32 query segments taken in Morton order (the sorted
+// leaves of the last rebuild), so a warp's queries are spatially close.  The warp walks the
+// tree as a packet: every step loads one node (the same address in all lanes), each lane tests
+// the node's two child boxes against its own query box, and the warp descends into a child if
+// any lane overlaps it (warp-uniform control flow, one shared stack).  A leaf that overlaps a
+// lane's box and has a larger segment index than the lane's becomes a candidate pair in a
+// per-warp queue; whenever 32 candidates are queued the warp runs the separately rounded
+// narrow-phase test on them, one pair per lane, and appends kept pairs to both lists.
+// Warps whose lanes all belong to one scene start at that scene's subtree root; the few
+// warps that straddle a scene boundary start at the global root and check leaf scenes.
 template <typename R>
 __global__ void __launch_bounds__(TRAV_THREADS) k_traverse(Dev<R> d) {
     __shared__ int sQ[TRAV_WARPS][TRAV_QCAP];
     __shared__ int sSeg[TRAV_WARPS][32];
     __shared__ int sScene[TRAV_WARPS][32];
+    __shared__ int sStack[TRAV_WARPS][BVH_STACK];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int si = blockIdx.x * blockDim.x + threadIdx.x;
-    int k = -1, node = -1, sc = 0;
+    const bool active = si < d.nseg;
+    int k = -1, sc = -1;
     Box<R> qb;
-    if (si < d.nseg) {
-        k = d.segs[si];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        qb.mn[a] = yinf<R>();
+        qb.mx[a] = -yinf<R>();
+    }
+    if (active) {
+        k = d.vals[0][si];
         sc = scene_of(d.vp[k].flags);
         qb = segment_box(d, k, d.sp[sc]);
-        node = d.sceneRoot[sc];
     }
     sSeg[warp][lane] = k;
     sScene[warp][lane] = sc;
-    bool done = node < 0;  // leaf root (one segment) or no query
-    int stack[BVH_STACK];
+    const unsigned actMask = __ballot_sync(0xffffffffu, active);
+    if (actMask == 0u || d.nseg < 2) return;  // (warp-uniform)
+    const int sc0 = __shfl_sync(0xffffffffu, sc, __ffs(actMask) - 1);
+    const bool mixed = !__all_sync(0xffffffffu, !active || sc == sc0);
+    int node = mixed ? 0 : d.sceneRoot[sc0];
+    bool done = node < 0;  // a scene of one segment has no pairs
     int top = 0;
     int qn = 0;  // queued candidates (identical in every lane)
     const unsigned lt = (1u << lane) - 1u;
@@ -252,34 +267,44 @@ __global__ void __launch_bounds__(TRAV_THREADS) k_traverse(Dev<R> d) {
     while (true) {
         int c0 = -1, c1 = -1;
         if (!done) {
-            const BNode<R>& nd = d.nodes[node];
-            bool ol = box_overlap(qb, nd.lmin, nd.lmax);
-            bool orr = box_overlap(qb, nd.rmin, nd.rmax);
+            BNode<R> nd;
+            if constexpr (sizeof(R) == 4) {  // one node = four 16-byte loads, same address in every lane
+                const float4* src = reinterpret_cast<const float4*>(d.nodes + node);
+                float4* dst = reinterpret_cast<float4*>(&nd);
+                dst[0] = __ldg(src); dst[1] = __ldg(src + 1); dst[2] = __ldg(src + 2); dst[3] = __ldg(src + 3);
+            } else {
+                nd = d.nodes[node];
+            }
+            const bool ol = box_overlap(qb, nd.lmin, nd.lmax);
+            const bool orr = box_overlap(qb, nd.rmin, nd.rmax);
             const int L = nd.left, Rc = nd.right;
-            if (ol && L < 0) {
-                if (-L - 1 > k) c0 = -L - 1;
-                ol = false;
+            if (ol && L < 0 && -L - 1 > k) c0 = -L - 1;
+            if (orr && Rc < 0 && -Rc - 1 > k) c1 = -Rc - 1;
+            if (mixed) {  // only warps at a scene boundary can see leaves of another scene
+                if (c0 >= 0 && scene_of(d.vp[c0].flags) != sc) c0 = -1;
+                if (c1 >= 0 && scene_of(d.vp[c1].flags) != sc) c1 = -1;
             }
-            if (orr && Rc < 0) {
-                if (-Rc - 1 > k) c1 = -Rc - 1;
-                orr = false;
-            }
-            if (ol && orr) {
+            const bool goL = __any_sync(0xffffffffu, ol && L >= 0);
+            const bool goR = __any_sync(0xffffffffu, orr && Rc >= 0);
+            if (goL && goR) {
                 if (top < BVH_STACK) {
-                    stack[top++] = Rc;
-                } else {
+                    if (lane == 0) sStack[warp][top] = Rc;
+                    top++;
+                } else if (lane == 0) {
                     atomicOr(&d.err[EW_INTERNAL], IE_BVH_STACK);
                 }
                 node = L;
-            } else if (ol) {
+            } else if (goL) {
                 node = L;
-            } else if (orr) {
+            } else if (goR) {
                 node = Rc;
             } else if (top > 0) {
-                node = stack[--top];
+                __syncwarp();
+                node = sStack[warp][--top];
             } else {
                 done = true;
             }
+            __syncwarp();
         }
         const unsigned b0 = __ballot_sync(0xffffffffu, c0 >= 0);
         const unsigned b1 = __ballot_sync(0xffffffffu, c1 >= 0);
@@ -287,8 +312,7 @@ __global__ void __launch_bounds__(TRAV_THREADS) k_traverse(Dev<R> d) {
         if (c1 >= 0) sQ[warp][qn + __popc(b0) + __popc(b1 & lt)] = (lane << TRAV_JBITS) | c1;
         qn += __popc(b0) + __popc(b1);
         __syncwarp();
-        const bool allDone = __all_sync(0xffffffffu, done);
-        while (qn >= 32 || (allDone && qn > 0)) {
+        while (qn >= 32 || (done && qn > 0)) {
             const int m = min(qn, 32);
             if (lane < m) {
                 const int e = sQ[warp][qn - m + lane];
@@ -303,7 +327,7 @@ __global__ void __launch_bounds__(TRAV_THREADS) k_traverse(Dev<R> d) {
             qn -= m;
             __syncwarp();
         }
-        if (allDone && qn == 0) break;
+        if (done && qn == 0) break;
     }
 }
 
