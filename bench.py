@@ -50,6 +50,11 @@ def parse():
     p.add_argument("--no-plain", action="store_true", help="skip the plain per-scene advance() loop")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     p.add_argument("--cap", type=int, default=8388608, help="vertex cap of the batched workload")
+    p.add_argument("--workload", default="batched", choices=["batched", "serve"])
+    p.add_argument("--rate", type=float, default=4.0, help="serve: Poisson arrival rate (requests/s)")
+    p.add_argument("--duration", type=float, default=10.0, help="serve: arrival window (s)")
+    p.add_argument("--frames", type=int, default=30, help="serve: frames per request")
+    p.add_argument("--budget-gb", type=float, default=120.0, help="serve: device-memory budget")
     return p.parse_args()
 
 
@@ -242,8 +247,8 @@ def run_ours(args):
     for _ in range(args.warmup):
         sim.advance(FRAME)
     # Autotuner: Newton-kernel shape (threads per block, lanes per vertex) timed on this state.
-    tune_threads, tune_lanes, tune_ms = sim.autotune()
-    cfg["newton_kernel_shape"] = {"threads": tune_threads, "lanes_per_vertex": tune_lanes,
+    tune_threads, tune_lanes, tune_pipe, tune_ms = sim.autotune()
+    cfg["newton_kernel_shape"] = {"threads": tune_threads, "lanes_per_vertex": tune_lanes, "pipelined": tune_pipe,
                                   "autotune_ms_per_launch": tune_ms}
     try:
         uuid = str(torch.cuda.get_device_properties(local).uuid)
@@ -323,7 +328,7 @@ def run_ours(args):
     pens = sim.penetrations()
     plain = None
     if not args.no_plain and rank == 0 and world == 1:
-        plain = run_plain(spec, stream, (tune_threads, tune_lanes))
+        plain = run_plain(spec, stream, (tune_threads, tune_lanes, tune_pipe))
     sim.close()
     cpu = None
     if not args.no_cpu and rank == 0 and world == 1:
@@ -370,7 +375,7 @@ def run_plain(spec, stream, shape):
         sm.maxH = MAX_H
         sm.upload()
         sm.set_stream(stream.cuda_stream)
-        sm.set_tuning(shape[0], shape[1], True)
+        sm.set_tuning(shape[0], shape[1], True, shape[2])
         sims.append(sm)
         off += counts[s]
     for sm in sims:
@@ -395,10 +400,75 @@ def run_plain(spec, stream, shape):
             "gpu_launches": int(launches), "scenes": len(sims)}
 
 
+def run_serve(args):
+    """Serving loop: Poisson arrivals in real time, continuous batching on one GPU, against
+    the same requests served one at a time (FIFO) through plain per-request advance()."""
+    import torch
+
+    from yarnball_b200 import serve
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    reqs = serve.poisson_requests(args.rate, args.duration, frames=args.frames)
+    server = serve.Server(budget_bytes=args.budget_gb * 1e9, shape=(128, 1), stream=torch.cuda.Stream())
+    pending = list(reqs)
+    t0 = time.perf_counter()
+    while pending or server.busy():
+        now = time.perf_counter() - t0
+        while pending and pending[0].arrival <= now:
+            server.submit(pending.pop(0))
+        if not server.busy() and pending:
+            time.sleep(max(0.0, pending[0].arrival - (time.perf_counter() - t0)))
+            continue
+        server.step(now)
+        done_t = time.perf_counter() - t0
+        for r in server.finished:
+            if r.finished_at is None:
+                r.finished_at = done_t
+    wall = time.perf_counter() - t0
+    server.close()
+    lat = [r.finished_at - r.arrival for r in reqs]
+    work = sum(r.vertices * SUBSTEPS * r.frames for r in reqs)
+    first, last = min(r.arrival for r in reqs), max(r.finished_at for r in reqs)
+    # the same requests, each alone, one after the other (FIFO single server)
+    service = []
+    for r in reqs:
+        sim = serve.build_request_sim(r, (128, 1))
+        st = torch.cuda.Stream()
+        sim.set_stream(st.cuda_stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(r.frames):
+            sim.advance(FRAME)
+        e1.record(st)
+        e1.synchronize()
+        service.append(e0.elapsed_time(e1) / 1e3)
+        sim.close()
+    tfree, lat_alone = 0.0, []
+    for r, sv in zip(reqs, service):
+        start = max(tfree, r.arrival)
+        tfree = start + sv
+        lat_alone.append(tfree - r.arrival)
+    out = {
+        "metric": "serving: request latency and vertex-substeps/s under Poisson arrivals", "unit": "s",
+        "requests": len(reqs), "rate_per_s": args.rate, "arrival_window_s": args.duration,
+        "frames_per_request": args.frames, "budget_gb": args.budget_gb,
+        "request_latency_s": serve.percentiles(lat), "frame_latency_ms": serve.percentiles(server.frame_ms),
+        "frames": len(server.frame_ms), "max_batch_vertices": max(server.frame_sizes) if server.frame_sizes else 0,
+        "gathers": server.gathers, "throughput_vertex_substeps_per_s": work / (last - first), "wall_s": wall,
+        "alone": {"request_latency_s": serve.percentiles(lat_alone),
+                  "throughput_vertex_substeps_per_s": work / (tfree - first),
+                  "service_s": serve.percentiles(service)},
+        "request_vertices": serve.percentiles([r.vertices for r in reqs]),
+    }
+    print(json.dumps(out))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "serve":
+        run_serve(args)
     else:
         run_ours(args)
 

@@ -174,15 +174,19 @@ const char* yb_status_string(yb_status s);
 
 /* ---- Additions without a reference counterpart ---------------------------------- */
 
-/* Engine tuning: threads per block of the Newton kernel and lanes per vertex (lanes split a
- * segment's contact loop: (128|256, 1), (256, 2), (256|512, 4), (256|512, 8)), and whether
- * substeps replay captured CUDA graphs.  Default (256, 4), graphs on. */
-yb_status yb_set_tuning(yb_sim* sim, int32_t iterThreads, int32_t lanesPerVertex, int32_t useGraphs);
-yb_status yb_get_tuning(yb_sim* sim, int32_t* iterThreads, int32_t* lanesPerVertex, int32_t* useGraphs);
+/* Engine tuning of the Newton kernel: threads per block, lanes per vertex (lanes split a
+ * segment's contact loop) and software pipelining of the contact loop; valid shapes:
+ * (128|256, 1, 0|1), (256, 2, 0), (256, 4, 0|1), (512, 4, 0), (256|512, 8, 0).  useGraphs: replay
+ * captured CUDA graphs per substep.  Default (256, 4, 0), graphs on. */
+yb_status yb_set_tuning(yb_sim* sim, int32_t iterThreads, int32_t lanesPerVertex, int32_t pipelined,
+                        int32_t useGraphs);
+yb_status yb_get_tuning(yb_sim* sim, int32_t* iterThreads, int32_t* lanesPerVertex, int32_t* pipelined,
+                        int32_t* useGraphs);
 
 /* Autotuner: times every Newton-kernel shape on the current device state (which it leaves
  * unchanged), keeps the fastest and returns it.  Call after at least one advance(). */
-yb_status yb_autotune(yb_sim* sim, int32_t* bestThreads, int32_t* bestLanes, float* bestMs);
+yb_status yb_autotune(yb_sim* sim, int32_t* bestThreads, int32_t* bestLanes, int32_t* bestPipelined,
+                      float* bestMs);
 
 /* Launch the simulation's work on `stream` (a cudaStream_t; NULL returns to the simulation's
  * own stream).  Lets a caller order the engine with its own work and time it with events. */
@@ -195,6 +199,27 @@ yb_status yb_set_stream(yb_sim* sim, void* stream);
  * iteration, 6 advection.  Arrays hold YB_PROFILE_CLASSES entries. */
 #define YB_PROFILE_CLASSES 7
 yb_status yb_profile_advance(yb_sim* sim, float dt, double* msByClass, uint64_t* launchesByClass);
+
+/* Continuous batching (no reference counterpart).  Builds a batch whose scene i is a copy of
+ * scene srcScenes[i] of srcSims[i], copying the device state device to device (nothing goes
+ * through the host); sources stay valid and unchanged.  If `recycle` is a batch with enough
+ * capacity (vertices and scenes) its device allocation is reused and *out == recycle;
+ * otherwise a new batch with room for max(total, capacityVerts) vertices is created and the
+ * caller still owns `recycle`.  The new batch starts with a BVH rebuild and a detection on
+ * its first substep, so a scene evolves identically alone and inside a batch when
+ * detectionPeriod is 1 and the Newton kernel shape is the same.  All sources must share a
+ * precision. */
+yb_status yb_batch_gather(int32_t count, yb_sim* const* srcSims, const int32_t* srcScenes, yb_sim* recycle,
+                          int64_t capacityVerts, yb_sim** out);
+
+/* download() restricted to one scene of a batch (its range of the host arrays). */
+yb_status yb_download_scene(yb_sim* sim, int32_t scene);
+
+/* First vertex and vertex count of a scene. */
+yb_status yb_scene_range(yb_sim* sim, int32_t scene, int32_t* first, int32_t* count);
+
+/* Device memory held by the simulation (bytes). */
+yb_status yb_device_bytes(yb_sim* sim, uint64_t* out);
 
 /* Kernels launched on the device so far (each graph node counts once per replay). */
 yb_status yb_launch_count(yb_sim* sim, uint64_t* out);

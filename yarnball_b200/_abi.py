@@ -102,10 +102,15 @@ SIGNATURES = {
     "yb_last_error": (ctypes.c_int, [_P, c_int32_p, c_int32_p]),
     "yb_initial_inv_masses": (ctypes.c_int, [_P, ctypes.POINTER(c_float_p), c_int32_p]),
     "yb_status_string": (ctypes.c_char_p, [ctypes.c_int]),
-    "yb_set_tuning": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
-    "yb_get_tuning": (ctypes.c_int, [_P, c_int32_p, c_int32_p, c_int32_p]),
-    "yb_autotune": (ctypes.c_int, [_P, c_int32_p, c_int32_p, c_float_p]),
+    "yb_set_tuning": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
+    "yb_get_tuning": (ctypes.c_int, [_P, c_int32_p, c_int32_p, c_int32_p, c_int32_p]),
+    "yb_autotune": (ctypes.c_int, [_P, c_int32_p, c_int32_p, c_int32_p, c_float_p]),
     "yb_launch_count": (ctypes.c_int, [_P, c_uint64_p]),
+    "yb_batch_gather": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(_P), c_int32_p, _P, ctypes.c_int64,
+                                       ctypes.POINTER(_P)]),
+    "yb_download_scene": (ctypes.c_int, [_P, ctypes.c_int32]),
+    "yb_device_bytes": (ctypes.c_int, [_P, c_uint64_p]),
+    "yb_scene_range": (ctypes.c_int, [_P, ctypes.c_int32, c_int32_p, c_int32_p]),
     "yb_set_stream": (ctypes.c_int, [_P, _P]),
     "yb_profile_advance": (ctypes.c_int, [_P, ctypes.c_float, c_double_p, c_uint64_p]),
     "yb_info": (ctypes.c_int, [_P, c_int32_p, c_int32_p, c_int32_p]),

@@ -123,7 +123,7 @@ struct Dev {
 // --- kernel launchers (stream-ordered; no host synchronisation) ---
 template <typename R> void launch_init(const Dev<R>& d, cudaStream_t s);
 template <typename R> void launch_end(const Dev<R>& d, int finalBuf, bool copyQ, bool kahan, cudaStream_t s);
-template <typename R> void launch_iter(const Dev<R>& d, int srcBuf, int threads, int lanes, cudaStream_t s);
+template <typename R> void launch_iter(const Dev<R>& d, int srcBuf, int threads, int lanes, int pipe, cudaStream_t s);
 template <typename R> void launch_bvh_rebuild(const Dev<R>& d, cudaStream_t s, void* sortScratch, size_t sortScratchBytes, int keyBits);
 template <typename R> void launch_bvh_refit(const Dev<R>& d, cudaStream_t s);
 template <typename R> void launch_traverse(const Dev<R>& d, cudaStream_t s);  // + list sort + step limit (2 kernels)

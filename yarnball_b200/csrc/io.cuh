@@ -6,7 +6,10 @@ namespace yb {
 template <typename R>
 void launch_convert_in(const Dev<R>& d, const void* hv, const float* hvel, const float* hq, const float* hqr,
                        const int* sceneOf, cudaStream_t s);
-template <typename R> void launch_convert_out(const Dev<R>& d, void* hv, float* hvel, float* hq, cudaStream_t s);
+// Converts vertices [first, first+count) to the host layout (written at the same offsets).
+template <typename R>
+void launch_convert_out(const Dev<R>& d, void* hv, float* hvel, float* hq, int first, int count, cudaStream_t s);
+template <typename R> void launch_relayout(const Dev<R>& d, const int* sceneOf, const int* delta, cudaStream_t s);
 template <typename R> void launch_zero_vel(const Dev<R>& d, cudaStream_t s);
 template <typename R>
 void launch_state_f64(const Dev<R>& d, int buf, double* pos, double* vel, double* q, double* dx, cudaStream_t s);

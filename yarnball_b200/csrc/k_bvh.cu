@@ -229,8 +229,8 @@ __device__ __forceinline__ void list_append(const Dev<R>& d, int x, int y) {
 // lane's box and has a larger segment index than the lane's becomes a candidate pair in a
 // per-warp queue; whenever 32 candidates are queued the warp runs the separately rounded
 // narrow-phase test on them, one pair per lane, and appends kept pairs to both lists.
-// Warps whose lanes all belong to one scene start at that scene's subtree root; the few
-// warps that straddle a scene boundary start at the global root and check leaf scenes.
+// A warp walks the subtree of its lanes' scene; the few warps that straddle a scene boundary
+// walk once per scene, each time with the other scene's lanes idle.
 template <typename R>
 __global__ void __launch_bounds__(TRAV_THREADS) k_traverse(Dev<R> d) {
     __shared__ int sQ[TRAV_WARPS][TRAV_QCAP];
@@ -254,16 +254,28 @@ __global__ void __launch_bounds__(TRAV_THREADS) k_traverse(Dev<R> d) {
     }
     sSeg[warp][lane] = k;
     sScene[warp][lane] = sc;
-    const unsigned actMask = __ballot_sync(0xffffffffu, active);
-    if (actMask == 0u || d.nseg < 2) return;  // (warp-uniform)
-    const int sc0 = __shfl_sync(0xffffffffu, sc, __ffs(actMask) - 1);
-    const bool mixed = !__all_sync(0xffffffffu, !active || sc == sc0);
-    int node = mixed ? 0 : d.sceneRoot[sc0];
+    unsigned todo = __ballot_sync(0xffffffffu, active);
+    if (todo == 0u || d.nseg < 2) return;  // (warp-uniform)
+    const unsigned lt = (1u << lane) - 1u;
+    int qn = 0;  // queued candidates (identical in every lane)
+    __syncwarp();
+    // One packet walk per distinct scene among the lanes (almost always one): lanes of other
+    // scenes take part with an empty query box.
+    while (todo) {
+    const int scw = __shfl_sync(0xffffffffu, sc, __ffs(todo) - 1);
+    const bool mine = active && sc == scw;
+    todo &= ~__ballot_sync(0xffffffffu, mine);
+    Box<R> pb = qb;
+    if (!mine) {
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            pb.mn[a] = yinf<R>();
+            pb.mx[a] = -yinf<R>();
+        }
+    }
+    int node = d.sceneRoot[scw];
     bool done = node < 0;  // a scene of one segment has no pairs
     int top = 0;
-    int qn = 0;  // queued candidates (identical in every lane)
-    const unsigned lt = (1u << lane) - 1u;
-    __syncwarp();
     while (true) {
         int c0 = -1, c1 = -1;
         if (!done) {
@@ -275,15 +287,11 @@ __global__ void __launch_bounds__(TRAV_THREADS) k_traverse(Dev<R> d) {
             } else {
                 nd = d.nodes[node];
             }
-            const bool ol = box_overlap(qb, nd.lmin, nd.lmax);
-            const bool orr = box_overlap(qb, nd.rmin, nd.rmax);
+            const bool ol = box_overlap(pb, nd.lmin, nd.lmax);
+            const bool orr = box_overlap(pb, nd.rmin, nd.rmax);
             const int L = nd.left, Rc = nd.right;
             if (ol && L < 0 && -L - 1 > k) c0 = -L - 1;
             if (orr && Rc < 0 && -Rc - 1 > k) c1 = -Rc - 1;
-            if (mixed) {  // only warps at a scene boundary can see leaves of another scene
-                if (c0 >= 0 && scene_of(d.vp[c0].flags) != sc) c0 = -1;
-                if (c1 >= 0 && scene_of(d.vp[c1].flags) != sc) c1 = -1;
-            }
             const bool goL = __any_sync(0xffffffffu, ol && L >= 0);
             const bool goR = __any_sync(0xffffffffu, orr && Rc >= 0);
             if (goL && goR) {
@@ -328,6 +336,7 @@ __global__ void __launch_bounds__(TRAV_THREADS) k_traverse(Dev<R> d) {
             __syncwarp();
         }
         if (done && qn == 0) break;
+    }
     }
 }
 

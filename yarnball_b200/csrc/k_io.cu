@@ -45,9 +45,11 @@ __global__ void k_convert_in(Dev<R> d, const HostVertex* __restrict__ hv, const 
 }
 
 template <typename R>
-__global__ void k_convert_out(Dev<R> d, HostVertex* __restrict__ hv, float* __restrict__ hvel, float* __restrict__ hq) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= d.n) return;
+__global__ void k_convert_out(Dev<R> d, HostVertex* __restrict__ hv, float* __restrict__ hvel, float* __restrict__ hq,
+                              int first, int count) {
+    const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ii >= count) return;
+    const int i = first + ii;
     const V4<R> p = d.pos[i];
     const VP<R> vp = d.vp[i];
     HostVertex v;
@@ -59,6 +61,22 @@ __global__ void k_convert_out(Dev<R> d, HostVertex* __restrict__ hv, float* __re
     hvel[3 * i] = (float)vel.x; hvel[3 * i + 1] = (float)vel.y; hvel[3 * i + 2] = (float)vel.z;
     const V4<R> q = d.q[0][i];
     hq[4 * i] = (float)q.x; hq[4 * i + 1] = (float)q.y; hq[4 * i + 2] = (float)q.z; hq[4 * i + 3] = (float)q.w;
+}
+
+// After scenes were copied into a new layout: scene ids in the flags, scene-boundary flags,
+// and connection indices shifted by each scene's offset change.
+template <typename R>
+__global__ void k_relayout(Dev<R> d, const int* __restrict__ sceneOf, const int* __restrict__ delta) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.n) return;
+    VP<R> vp = d.vp[i];
+    const int sc = sceneOf[i];
+    uint32_t fl = vp.flags & F_USER_MASK;
+    if (i == d.n - 1 || sceneOf[i + 1] != sc) fl &= ~(uint32_t)(F_HAS_NEXT | F_HAS_NEXT_ORI);
+    if (i == 0 || sceneOf[i - 1] != sc) fl &= ~(uint32_t)F_HAS_PREV;
+    vp.flags = fl | ((uint32_t)sc << 8);
+    if (vp.cid >= 0) vp.cid += delta[sc];
+    d.vp[i] = vp;
 }
 
 template <typename R>
@@ -191,9 +209,14 @@ void launch_convert_in(const Dev<R>& d, const void* hv, const float* hvel, const
     k_convert_in<R><<<(d.n + 255) / 256, 256, 0, s>>>(d, (const HostVertex*)hv, hvel, hq, hqr, sceneOf);
 }
 template <typename R>
-void launch_convert_out(const Dev<R>& d, void* hv, float* hvel, float* hq, cudaStream_t s) {
+void launch_convert_out(const Dev<R>& d, void* hv, float* hvel, float* hq, int first, int count, cudaStream_t s) {
+    if (count <= 0) return;
+    k_convert_out<R><<<(count + 255) / 256, 256, 0, s>>>(d, (HostVertex*)hv, hvel, hq, first, count);
+}
+template <typename R>
+void launch_relayout(const Dev<R>& d, const int* sceneOf, const int* delta, cudaStream_t s) {
     if (d.n <= 0) return;
-    k_convert_out<R><<<(d.n + 255) / 256, 256, 0, s>>>(d, (HostVertex*)hv, hvel, hq);
+    k_relayout<R><<<(d.n + 255) / 256, 256, 0, s>>>(d, sceneOf, delta);
 }
 template <typename R>
 void launch_zero_vel(const Dev<R>& d, cudaStream_t s) {
@@ -219,7 +242,8 @@ int launch_diag(const Dev<R>& d, double* part, cudaStream_t s) {
 #define YB_INST(R)                                                                                          \
     template void launch_convert_in<R>(const Dev<R>&, const void*, const float*, const float*, const float*, \
                                        const int*, cudaStream_t);                                            \
-    template void launch_convert_out<R>(const Dev<R>&, void*, float*, float*, cudaStream_t);                 \
+    template void launch_convert_out<R>(const Dev<R>&, void*, float*, float*, int, int, cudaStream_t);       \
+    template void launch_relayout<R>(const Dev<R>&, const int*, const int*, cudaStream_t);                   \
     template void launch_zero_vel<R>(const Dev<R>&, cudaStream_t);                                           \
     template void launch_state_f64<R>(const Dev<R>&, int, double*, double*, double*, double*, cudaStream_t); \
     template void launch_scene_root_box<R>(const Dev<R>&, float*, cudaStream_t);                             \

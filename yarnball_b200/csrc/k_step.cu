@@ -171,7 +171,7 @@ __device__ __forceinline__ R slot_sum(R v) {
     return v;
 }
 
-template <typename R, int NT, int T, int MINB>
+template <typename R, int NT, int T, int MINB, bool PIPE>
 __global__ void __launch_bounds__(NT, MINB) k_iter(Dev<R> d, int src) {
     constexpr int B = NT / T;
     constexpr int CORE = B - 2;
@@ -249,24 +249,67 @@ __global__ void __launch_bounds__(NT, MINB) k_iter(Dev<R> d, int src) {
             // Barrier + friction over this lane's share of the contact list.  Partner
             // positions relative to p0 are staged per substep for the first RELCAP contacts;
             // the partner's iterate pair is one 32-byte gather.
+            // With PIPE the loads of the lane's next contact are issued before the current
+            // contact's arithmetic, so the dependent partner gather overlaps it (more
+            // registers); without it each contact loads then computes.
             const int nc = d.numCols[k];
             const int* __restrict__ cl = d.cols + k;
             const V3<R> e = p1 - p0;
-            for (int c2 = lane; c2 < nc; c2 += T) {
+            if constexpr (!PIPE) {
+                for (int c2 = lane; c2 < nc; c2 += T) {
+                    const size_t at = k + (size_t)n * c2;
+                    const int j = __ldg(cl + (size_t)n * c2);
+                    V3<R> r0, r1;
+                    if (c2 < RELCAP) {
+                        const V4<R> A = d.relA[at];
+                        const R2<R> Bq = d.relB[at];
+                        r0 = V3<R>(A.x, A.y, A.z);
+                        r1 = V3<R>(A.w, Bq.x, Bq.y);
+                    } else {
+                        r0 = xyz(d.pos[j]) - p0;
+                        r1 = xyz(d.pos[j + 1]) - p0;
+                    }
+                    const D2<R> pd = DX[j];
+                    contact_term(e, dx, dx1, r0, r1, xyz(pd.a), xyz(pd.b), sp, fa, Ha, fb, Hb);
+                }
+            } else {
+            int c2 = lane;
+            V3<R> r0n(R(0)), r1n(R(0));
+            D2<R> pdn;
+            if (c2 < nc) {
                 const size_t at = k + (size_t)n * c2;
                 const int j = __ldg(cl + (size_t)n * c2);
-                V3<R> r0, r1;
                 if (c2 < RELCAP) {
                     const V4<R> A = d.relA[at];
                     const R2<R> Bq = d.relB[at];
-                    r0 = V3<R>(A.x, A.y, A.z);
-                    r1 = V3<R>(A.w, Bq.x, Bq.y);
+                    r0n = V3<R>(A.x, A.y, A.z);
+                    r1n = V3<R>(A.w, Bq.x, Bq.y);
                 } else {
-                    r0 = xyz(d.pos[j]) - p0;
-                    r1 = xyz(d.pos[j + 1]) - p0;
+                    r0n = xyz(d.pos[j]) - p0;
+                    r1n = xyz(d.pos[j + 1]) - p0;
                 }
-                const D2<R> pd = DX[j];
+                pdn = DX[j];
+            }
+            while (c2 < nc) {
+                const V3<R> r0 = r0n, r1 = r1n;
+                const D2<R> pd = pdn;
+                c2 += T;
+                if (c2 < nc) {
+                    const size_t at = k + (size_t)n * c2;
+                    const int j = __ldg(cl + (size_t)n * c2);
+                    if (c2 < RELCAP) {
+                        const V4<R> A = d.relA[at];
+                        const R2<R> Bq = d.relB[at];
+                        r0n = V3<R>(A.x, A.y, A.z);
+                        r1n = V3<R>(A.w, Bq.x, Bq.y);
+                    } else {
+                        r0n = xyz(d.pos[j]) - p0;
+                        r1n = xyz(d.pos[j + 1]) - p0;
+                    }
+                    pdn = DX[j];
+                }
                 contact_term(e, dx, dx1, r0, r1, xyz(pd.a), xyz(pd.b), sp, fa, Ha, fb, Hb);
+            }
             }
         }
     }
@@ -358,20 +401,24 @@ void launch_end(const Dev<R>& d, int finalBuf, bool copyQ, bool kahan, cudaStrea
     k_end<R><<<(d.n + 255) / 256, 256, 0, s>>>(d, finalBuf, copyQ ? 1 : 0, kahan ? 1 : 0);
 }
 
-// Newton iteration launch shapes: NT threads per block, T lanes per vertex.
+// Newton iteration launch shapes: NT threads per block, T lanes per vertex, pipelined or not.
 template <typename R>
-void launch_iter(const Dev<R>& d, int srcBuf, int threads, int lanes, cudaStream_t s) {
+void launch_iter(const Dev<R>& d, int srcBuf, int threads, int lanes, int pipe, cudaStream_t s) {
     if (d.n <= 0) return;
-#define YB_ITER(NT, T, MINB) \
-    k_iter<R, NT, T, MINB><<<(d.n + (NT / T) - 3) / ((NT / T) - 2), NT, 0, s>>>(d, srcBuf)
-    if (lanes == 2) {
-        YB_ITER(256, 2, 3);
+#define YB_ITER(NT, T, MINB, P) \
+    k_iter<R, NT, T, MINB, P><<<(d.n + (NT / T) - 3) / ((NT / T) - 2), NT, 0, s>>>(d, srcBuf)
+    if (pipe) {
+        if (lanes == 4) YB_ITER(256, 4, 2, true);
+        else if (threads == 128) YB_ITER(128, 1, 4, true);
+        else YB_ITER(256, 1, 2, true);
+    } else if (lanes == 2) {
+        YB_ITER(256, 2, 3, false);
     } else if (lanes == 4) {
-        if (threads == 512) YB_ITER(512, 4, 2); else YB_ITER(256, 4, 3);
+        if (threads == 512) YB_ITER(512, 4, 2, false); else YB_ITER(256, 4, 3, false);
     } else if (lanes == 8) {
-        if (threads == 512) YB_ITER(512, 8, 2); else YB_ITER(256, 8, 3);
+        if (threads == 512) YB_ITER(512, 8, 2, false); else YB_ITER(256, 8, 3, false);
     } else {
-        if (threads == 128) YB_ITER(128, 1, 6); else YB_ITER(256, 1, 2);
+        if (threads == 128) YB_ITER(128, 1, 6, false); else YB_ITER(256, 1, 2, false);
     }
 #undef YB_ITER
 }
@@ -380,7 +427,7 @@ template void launch_init<float>(const Dev<float>&, cudaStream_t);
 template void launch_init<double>(const Dev<double>&, cudaStream_t);
 template void launch_end<float>(const Dev<float>&, int, bool, bool, cudaStream_t);
 template void launch_end<double>(const Dev<double>&, int, bool, bool, cudaStream_t);
-template void launch_iter<float>(const Dev<float>&, int, int, int, cudaStream_t);
-template void launch_iter<double>(const Dev<double>&, int, int, int, cudaStream_t);
+template void launch_iter<float>(const Dev<float>&, int, int, int, int, cudaStream_t);
+template void launch_iter<double>(const Dev<double>&, int, int, int, int, cudaStream_t);
 
 }  // namespace yb

@@ -50,7 +50,10 @@ struct EngineBase {
     virtual uint64_t debug_phases(int mask, int& buf) = 0;
     virtual int64_t penetrations() = 0;
     virtual yb_status profile_substep(bool detect, bool rebuild, double* ms, uint64_t* launches) = 0;
-    virtual yb_status time_iter(int threads, int lanes, int reps, float* ms) = 0;
+    virtual yb_status time_iter(int threads, int lanes, int pipe, int reps, float* ms) = 0;
+    virtual yb_status download_range(int first, int count) = 0;
+    virtual yb_status gather(int count, yb_sim* const* src, const int* srcScenes) = 0;
+    virtual size_t device_bytes() const = 0;
 };
 
 }  // namespace
@@ -58,6 +61,8 @@ struct EngineBase {
 struct yb_sim {
     int n = 0;
     int numScenes = 1;
+    int capVerts = 0;   // host arrays and device buffers hold this many vertices
+    int capScenes = 0;  // ... and this many scenes (a recycled batch may use fewer)
     int precision = YB_PRECISION_FP32;
     std::vector<int> sceneOff;  // numScenes + 1
     std::vector<yb_meta> meta;  // per scene
@@ -74,6 +79,7 @@ struct yb_sim {
     int lastErrorCode = 0, lastWarningCode = 0;
     int iterThreads = 256;
     int iterLanes = 4;
+    int iterPipe = 0;
     int useGraphs = 1;
     uint64_t launches = 0;
     cudaStream_t stream = nullptr;     // active stream (own or the caller's)
@@ -280,12 +286,13 @@ struct Engine : EngineBase {
     char* stage = nullptr;  // host-layout staging: verts | vels | qs | qRests
     float* rootBoxes = nullptr;
     double* diagPart = nullptr;
+    int* sceneDelta = nullptr;
     SceneParams<R>* spDev = nullptr;
     SceneParams<R>* spHost = nullptr;
     int* errHost = nullptr;
     cudaGraphExec_t graphs[GRAPH_TYPES] = {nullptr, nullptr, nullptr};
     uint64_t graphLaunches[GRAPH_TYPES] = {0, 0, 0};
-    int graphItr = -1, graphThreads = -1, graphLanes = -1, graphNseg = -1;
+    int graphItr = -1, graphThreads = -1, graphLanes = -1, graphPipe = -1, graphNseg = -1;
     int keyBits = 30;
     int64_t penTotal = 0;
 
@@ -299,9 +306,11 @@ struct Engine : EngineBase {
         if (errHost) cudaFreeHost(errHost);
     }
 
+    size_t allocBytes = 0;
+
     yb_status alloc() {
-        const size_t n = (size_t)S->n;
-        const size_t ns = (size_t)S->numScenes;
+        const size_t n = (size_t)S->capVerts;
+        const size_t ns = (size_t)S->capScenes;
         const size_t nn = n > 1 ? n - 1 : 1;
         sortBytes = radix_sort_scratch_bytes((int)n);
         size_t off = 0;
@@ -339,8 +348,10 @@ struct Engine : EngineBase {
         want((void**)&stage, (sizeof(yb_vertex) + 12 + 16 + 16) * n);
         want((void**)&rootBoxes, sizeof(float) * 6 * ns);
         want((void**)&diagPart, sizeof(double) * 8 * ((n + 255) / 256 + 1));
+        want((void**)&sceneDelta, sizeof(int) * ns);
         for (auto& r : req) off += (r.second + 255) & ~(size_t)255;
         YB_CUDA(cudaMalloc(&block, off));
+        allocBytes = off;
         off = 0;
         for (auto& r : req) {
             *r.first = (char*)block + off;
@@ -357,18 +368,97 @@ struct Engine : EngineBase {
         YB_CUDA(cudaMemsetAsync(d.numCols, 0, sizeof(int) * n, S->stream));
         YB_CUDA(cudaMemsetAsync(d.lastVel, 0, sizeof(V4<R>) * n, S->stream));
         YB_CUDA(cudaMemsetAsync(d.refitCount, 0, sizeof(unsigned) * nn, S->stream));
-        std::vector<int> so(n);
-        for (int s = 0; s < S->numScenes; s++)
-            for (int i = S->sceneOff[s]; i < S->sceneOff[s + 1]; i++) so[i] = s;
-        YB_CUDA(cudaMemcpyAsync(sceneOf, so.data(), sizeof(int) * n, cudaMemcpyHostToDevice, S->stream));
+        YB_CUDA(upload_layout());
         launch_bvh_reset(d, S->stream);
-        keyBits = 30 + scene_bits(S->numScenes);
         YB_CUDA(cudaStreamSynchronize(S->stream));
         return YB_OK;
     }
 
+    // Scene of every vertex and the sort key width for the current scene layout.
+    cudaError_t upload_layout() {
+        std::vector<int> so((size_t)S->n);
+        for (int s = 0; s < S->numScenes; s++)
+            for (int i = S->sceneOff[s]; i < S->sceneOff[s + 1]; i++) so[i] = s;
+        d.n = S->n;
+        d.numScenes = S->numScenes;
+        keyBits = 30 + scene_bits(S->numScenes);
+        cudaError_t e = cudaMemcpyAsync(sceneOf, so.data(), sizeof(int) * so.size(), cudaMemcpyHostToDevice, S->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(S->stream);
+        return e;
+    }
+
+    size_t device_bytes() const override { return allocBytes; }
+
+    // Segment list from the host flags (the rule of upload()).
+    yb_status refresh_segments() {
+        std::vector<int> segs;
+        segs.reserve((size_t)S->n);
+        for (int s = 0; s < S->numScenes; s++)
+            for (int i = S->sceneOff[s]; i + 1 < S->sceneOff[s + 1]; i++)
+                if (has(S->verts[i].flags, YB_HAS_NEXT)) segs.push_back(i);
+        if (!segs.empty())
+            YB_CUDA(cudaMemcpyAsync(d.segs, segs.data(), sizeof(int) * segs.size(), cudaMemcpyHostToDevice, S->stream));
+        YB_CUDA(cudaStreamSynchronize(S->stream));
+        d.nseg = (int)segs.size();
+        S->segs.swap(segs);
+        S->lastBVHRebuild = INFINITY;
+        invalidate_graphs();
+        return YB_OK;
+    }
+
+    yb_status download_range(int first, int count) override {
+        char* sv = stage;
+        char* svel = sv + sizeof(yb_vertex) * (size_t)S->capVerts;
+        char* sq = svel + 12 * (size_t)S->capVerts;
+        cudaStream_t st = S->stream;
+        launch_convert_out(d, sv, (float*)svel, (float*)sq, first, count, st);
+        S->launches++;
+        YB_CUDA(cudaGetLastError());
+        YB_CUDA(cudaMemcpyAsync(S->verts + first, sv + sizeof(yb_vertex) * first, sizeof(yb_vertex) * count,
+                                cudaMemcpyDeviceToHost, st));
+        YB_CUDA(cudaMemcpyAsync(S->vels + 3 * (size_t)first, svel + 12 * (size_t)first, 12 * (size_t)count,
+                                cudaMemcpyDeviceToHost, st));
+        YB_CUDA(cudaMemcpyAsync(S->qs + 4 * (size_t)first, sq + 16 * (size_t)first, 16 * (size_t)count,
+                                cudaMemcpyDeviceToHost, st));
+        YB_CUDA(cudaStreamSynchronize(st));
+        return YB_OK;
+    }
+
+    // Copies scene srcScenes[i] of src[i] into scene i of this simulation's current layout
+    // (device to device), then fixes scene ids and connection indices.
+    yb_status gather(int count, yb_sim* const* src, const int* srcScenes) override {
+        cudaStream_t st = S->stream;
+        YB_CUDA(upload_layout());
+        std::vector<int> delta(count);
+        for (int i = 0; i < count; i++) {
+            yb_sim* Sx = src[i];
+            YB_CUDA(cudaStreamSynchronize(Sx->stream));
+            const Dev<R>& sd = static_cast<Engine<R>*>(Sx->eng)->d;
+            const size_t so = (size_t)Sx->sceneOff[srcScenes[i]];
+            const size_t m = (size_t)(Sx->sceneOff[srcScenes[i] + 1] - Sx->sceneOff[srcScenes[i]]);
+            const size_t to = (size_t)S->sceneOff[i];
+            delta[i] = (int)to - (int)so;
+            const size_t v4b = sizeof(V4<R>) * m;
+            YB_CUDA(cudaMemcpyAsync(d.pos + to, sd.pos + so, v4b, cudaMemcpyDeviceToDevice, st));
+            YB_CUDA(cudaMemcpyAsync(d.posC + to, sd.posC + so, v4b, cudaMemcpyDeviceToDevice, st));
+            YB_CUDA(cudaMemcpyAsync(d.vel + to, sd.vel + so, v4b, cudaMemcpyDeviceToDevice, st));
+            YB_CUDA(cudaMemcpyAsync(d.lastVel + to, sd.lastVel + so, v4b, cudaMemcpyDeviceToDevice, st));
+            YB_CUDA(cudaMemcpyAsync(d.q[0] + to, sd.q[0] + so, v4b, cudaMemcpyDeviceToDevice, st));
+            YB_CUDA(cudaMemcpyAsync(d.qRest + to, sd.qRest + so, v4b, cudaMemcpyDeviceToDevice, st));
+            YB_CUDA(cudaMemcpyAsync(d.vp + to, sd.vp + so, sizeof(VP<R>) * m, cudaMemcpyDeviceToDevice, st));
+        }
+        YB_CUDA(cudaMemcpyAsync(sceneDelta, delta.data(), sizeof(int) * count, cudaMemcpyHostToDevice, st));
+        launch_relayout(d, sceneOf, sceneDelta, st);
+        S->launches++;
+        YB_CUDA(cudaMemsetAsync(d.numCols, 0, sizeof(int) * (size_t)S->n, st));
+        YB_CUDA(cudaGetLastError());
+        YB_CUDA(cudaStreamSynchronize(st));
+        return refresh_segments();
+    }
+
     yb_status upload() override {
         const size_t n = (size_t)S->n;
+        const size_t cap = (size_t)S->capVerts;
         // Segment list and connection validation from the host flags.
         std::vector<int> segs;
         segs.reserve(n);
@@ -380,9 +470,9 @@ struct Engine : EngineBase {
             }
         }
         char* sv = stage;
-        char* svel = sv + sizeof(yb_vertex) * n;
-        char* sq = svel + 12 * n;
-        char* sqr = sq + 16 * n;
+        char* svel = sv + sizeof(yb_vertex) * cap;
+        char* sq = svel + 12 * cap;
+        char* sqr = sq + 16 * cap;
         cudaStream_t st = S->stream;
         YB_CUDA(cudaMemcpyAsync(sv, S->verts, sizeof(yb_vertex) * n, cudaMemcpyHostToDevice, st));
         YB_CUDA(cudaMemcpyAsync(svel, S->vels, 12 * n, cudaMemcpyHostToDevice, st));
@@ -406,10 +496,10 @@ struct Engine : EngineBase {
     yb_status download() override {
         const size_t n = (size_t)S->n;
         char* sv = stage;
-        char* svel = sv + sizeof(yb_vertex) * n;
-        char* sq = svel + 12 * n;
+        char* svel = sv + sizeof(yb_vertex) * (size_t)S->capVerts;
+        char* sq = svel + 12 * (size_t)S->capVerts;
         cudaStream_t st = S->stream;
-        launch_convert_out(d, sv, (float*)svel, (float*)sq, st);
+        launch_convert_out(d, sv, (float*)svel, (float*)sq, 0, S->n, st);
         S->launches++;
         YB_CUDA(cudaGetLastError());
         YB_CUDA(cudaMemcpyAsync(S->verts, sv, sizeof(yb_vertex) * n, cudaMemcpyDeviceToHost, st));
@@ -457,7 +547,7 @@ struct Engine : EngineBase {
         }
         const int I = num_itr();
         for (int it = 0; it < I; it++) {
-            launch_iter(d, it & 1, S->iterThreads, S->iterLanes, st);
+            launch_iter(d, it & 1, S->iterThreads, S->iterLanes, S->iterPipe, st);
             k++;
         }
         launch_end(d, I & 1, (I & 1) != 0, sizeof(R) == 4, st); k++;
@@ -469,7 +559,7 @@ struct Engine : EngineBase {
             if (g) cudaGraphExecDestroy(g);
             g = nullptr;
         }
-        graphItr = graphThreads = graphLanes = graphNseg = -1;
+        graphItr = graphThreads = graphLanes = graphPipe = graphNseg = -1;
     }
 
     yb_status run_substep(int type) override {
@@ -480,11 +570,12 @@ struct Engine : EngineBase {
             return YB_OK;
         }
         if (graphItr != num_itr() || graphThreads != S->iterThreads || graphLanes != S->iterLanes ||
-            graphNseg != d.nseg) {
+            graphPipe != S->iterPipe || graphNseg != d.nseg) {
             invalidate_graphs();
             graphItr = num_itr();
             graphThreads = S->iterThreads;
             graphLanes = S->iterLanes;
+            graphPipe = S->iterPipe;
             graphNseg = d.nseg;
         }
         if (!graphs[type]) {
@@ -631,7 +722,7 @@ struct Engine : EngineBase {
             launch_lists_step_limit(d, st); launches[4]++;
         }
         mark(5);
-        for (int it = 0; it < I; it++) launch_iter(d, it & 1, S->iterThreads, S->iterLanes, st);
+        for (int it = 0; it < I; it++) launch_iter(d, it & 1, S->iterThreads, S->iterLanes, S->iterPipe, st);
         launches[5] += I;
         mark(6);
         launch_end(d, I & 1, (I & 1) != 0, sizeof(R) == 4, st); launches[6]++;
@@ -651,14 +742,14 @@ struct Engine : EngineBase {
     // Average device time of one Newton iteration launch of the given shape on the current
     // state.  Reads dx[0]/q[0] and writes only dx[1]/q[1], which hold nothing between
     // substeps, so the simulation state is unchanged.
-    yb_status time_iter(int threads, int lanes, int reps, float* ms) override {
+    yb_status time_iter(int threads, int lanes, int pipe, int reps, float* ms) override {
         cudaStream_t st = S->stream;
         cudaEvent_t e0, e1;
         YB_CUDA(cudaEventCreate(&e0));
         YB_CUDA(cudaEventCreate(&e1));
-        launch_iter(d, 0, threads, lanes, st);
+        launch_iter(d, 0, threads, lanes, pipe, st);
         cudaEventRecord(e0, st);
-        for (int r = 0; r < reps; r++) launch_iter(d, 0, threads, lanes, st);
+        for (int r = 0; r < reps; r++) launch_iter(d, 0, threads, lanes, pipe, st);
         cudaEventRecord(e1, st);
         S->launches += reps + 1;
         cudaError_t e = cudaGetLastError();
@@ -682,7 +773,7 @@ struct Engine : EngineBase {
             k += 3;
         }
         if (mask & 8) { launch_lists_step_limit(d, st); k++; }
-        if (mask & 16) { launch_iter(d, buf, S->iterThreads, S->iterLanes, st); buf ^= 1; k++; }
+        if (mask & 16) { launch_iter(d, buf, S->iterThreads, S->iterLanes, S->iterPipe, st); buf ^= 1; k++; }
         if (mask & 32) { launch_end(d, buf, buf != 0, sizeof(R) == 4, st); buf = 0; k++; }
         return k;
     }
@@ -711,7 +802,15 @@ yb_status validate_all_meta(yb_sim* S) {
 // =========================================================================================
 extern "C" {
 
+static yb_status create_internal(int32_t numScenes, const int32_t* vertsPerScene, int32_t precision,
+                                 long long capVerts, int32_t capScenes, yb_sim** out);
+
 yb_status yb_create_batch(int32_t numScenes, const int32_t* vertsPerScene, int32_t precision, yb_sim** out) {
+    return create_internal(numScenes, vertsPerScene, precision, 0, 0, out);
+}
+
+static yb_status create_internal(int32_t numScenes, const int32_t* vertsPerScene, int32_t precision,
+                                 long long capVerts, int32_t capScenes, yb_sim** out) {
     if (!out || numScenes < 1 || !vertsPerScene) return YB_ERR_INVALID_ARGUMENT;
     if (precision != YB_PRECISION_FP32 && precision != YB_PRECISION_FP64) return YB_ERR_INVALID_ARGUMENT;
     *out = nullptr;
@@ -720,17 +819,21 @@ yb_status yb_create_batch(int32_t numScenes, const int32_t* vertsPerScene, int32
         if (vertsPerScene[s] < 3) return YB_ERR_TOO_FEW_VERTICES;
         total += vertsPerScene[s];
     }
-    if (total > (1LL << 31) / YB_MAX_COLLISIONS_PER_SEGMENT) return YB_ERR_INVALID_ARGUMENT;
+    if (capVerts < total) capVerts = total;
+    if (capScenes < numScenes) capScenes = numScenes;
+    if (capVerts > (1LL << 31) / YB_MAX_COLLISIONS_PER_SEGMENT) return YB_ERR_INVALID_ARGUMENT;
     yb_sim* S = new (std::nothrow) yb_sim();
     if (!S) return YB_ERR_OUT_OF_MEMORY;
     S->n = (int)total;
     S->numScenes = numScenes;
+    S->capVerts = (int)capVerts;
+    S->capScenes = capScenes;
     S->precision = precision;
     S->sceneOff.resize(numScenes + 1, 0);
     for (int s = 0; s < numScenes; s++) S->sceneOff[s + 1] = S->sceneOff[s] + vertsPerScene[s];
     S->meta.resize(numScenes);
     for (int s = 0; s < numScenes; s++) default_meta(S->meta[s], vertsPerScene[s], S->maxH);
-    const size_t n = (size_t)total;
+    const size_t n = (size_t)capVerts;
     const size_t bytes = n * (sizeof(yb_vertex) + 12 + 16 + 16);
     void* host = nullptr;
     if (cudaHostAlloc(&host, bytes, cudaHostAllocDefault) == cudaSuccess) {
@@ -765,7 +868,7 @@ yb_status yb_create_batch(int32_t numScenes, const int32_t* vertsPerScene, int32
 }
 
 yb_status yb_create(int32_t numVerts, yb_sim** out) {
-    return yb_create_batch(1, &numVerts, YB_PRECISION_FP32, out);
+    return create_internal(1, &numVerts, YB_PRECISION_FP32, 0, 0, out);
 }
 
 void yb_destroy(yb_sim* S) {
@@ -1006,48 +1109,55 @@ const char* yb_status_string(yb_status s) {
     return "unknown status";
 }
 
-static bool valid_shape(int threads, int lanes) {
+static bool valid_shape(int threads, int lanes, int pipe) {
+    if (pipe) return (lanes == 1 && (threads == 128 || threads == 256)) || (lanes == 4 && threads == 256);
     return (lanes == 1 && (threads == 128 || threads == 256)) || (lanes == 2 && threads == 256) ||
            ((lanes == 4 || lanes == 8) && (threads == 256 || threads == 512));
 }
 
-yb_status yb_set_tuning(yb_sim* S, int32_t iterThreads, int32_t lanesPerVertex, int32_t useGraphs) {
-    if (!S || !valid_shape(iterThreads, lanesPerVertex)) return YB_ERR_INVALID_ARGUMENT;
+yb_status yb_set_tuning(yb_sim* S, int32_t iterThreads, int32_t lanesPerVertex, int32_t pipelined, int32_t useGraphs) {
+    if (!S || !valid_shape(iterThreads, lanesPerVertex, pipelined)) return YB_ERR_INVALID_ARGUMENT;
     S->iterThreads = iterThreads;
     S->iterLanes = lanesPerVertex;
+    S->iterPipe = pipelined ? 1 : 0;
     S->useGraphs = useGraphs ? 1 : 0;
     if (S->eng) S->eng->invalidate_graphs();
     return YB_OK;
 }
 
-yb_status yb_get_tuning(yb_sim* S, int32_t* iterThreads, int32_t* lanesPerVertex, int32_t* useGraphs) {
+yb_status yb_get_tuning(yb_sim* S, int32_t* iterThreads, int32_t* lanesPerVertex, int32_t* pipelined,
+                        int32_t* useGraphs) {
     if (!S) return YB_ERR_INVALID_ARGUMENT;
     if (iterThreads) *iterThreads = S->iterThreads;
     if (lanesPerVertex) *lanesPerVertex = S->iterLanes;
+    if (pipelined) *pipelined = S->iterPipe;
     if (useGraphs) *useGraphs = S->useGraphs;
     return YB_OK;
 }
 
-yb_status yb_autotune(yb_sim* S, int32_t* bestThreads, int32_t* bestLanes, float* bestMs) {
+yb_status yb_autotune(yb_sim* S, int32_t* bestThreads, int32_t* bestLanes, int32_t* bestPipelined, float* bestMs) {
     if (!S) return YB_ERR_INVALID_ARGUMENT;
     if (!S->configured) return YB_ERR_NOT_CONFIGURED;
-    static const int shapes[][2] = {{256, 1}, {128, 1}, {256, 2}, {256, 4}, {512, 4}, {256, 8}, {512, 8}};
+    static const int shapes[][3] = {{256, 1, 0}, {128, 1, 0}, {256, 2, 0}, {256, 4, 0}, {512, 4, 0}, {256, 8, 0},
+                                    {512, 8, 0}, {128, 1, 1}, {256, 1, 1}, {256, 4, 1}};
     float best = INFINITY;
-    int bt = S->iterThreads, bl = S->iterLanes;
+    int bt = S->iterThreads, bl = S->iterLanes, bp = S->iterPipe;
     S->eng->write_params();
     for (const auto& sh : shapes) {
         float ms = 0.f;
-        const yb_status st = S->eng->time_iter(sh[0], sh[1], 5, &ms);
+        const yb_status st = S->eng->time_iter(sh[0], sh[1], sh[2], 5, &ms);
         if (st != YB_OK) return st;
         if (ms < best) {
             best = ms;
             bt = sh[0];
             bl = sh[1];
+            bp = sh[2];
         }
     }
-    const yb_status st = yb_set_tuning(S, bt, bl, S->useGraphs);
+    const yb_status st = yb_set_tuning(S, bt, bl, bp, S->useGraphs);
     if (bestThreads) *bestThreads = bt;
     if (bestLanes) *bestLanes = bl;
+    if (bestPipelined) *bestPipelined = bp;
     if (bestMs) *bestMs = best;
     return st;
 }
@@ -1094,6 +1204,104 @@ yb_status yb_profile_advance(yb_sim* S, float dt, double* msByClass, uint64_t* l
     }
     for (auto& m : S->meta) m.time += dt;
     return S->eng->check_errors();
+}
+
+yb_status yb_download_scene(yb_sim* S, int32_t scene) {
+    if (!S || scene < 0 || scene >= S->numScenes) return YB_ERR_INVALID_ARGUMENT;
+    if (!S->configured) return YB_ERR_NOT_CONFIGURED;
+    return S->eng->download_range(S->sceneOff[scene], S->sceneOff[scene + 1] - S->sceneOff[scene]);
+}
+
+yb_status yb_scene_range(yb_sim* S, int32_t scene, int32_t* first, int32_t* count) {
+    if (!S || scene < 0 || scene >= S->numScenes) return YB_ERR_INVALID_ARGUMENT;
+    if (first) *first = S->sceneOff[scene];
+    if (count) *count = S->sceneOff[scene + 1] - S->sceneOff[scene];
+    return YB_OK;
+}
+
+yb_status yb_device_bytes(yb_sim* S, uint64_t* out) {
+    if (!S || !out) return YB_ERR_INVALID_ARGUMENT;
+    *out = S->eng ? (uint64_t)S->eng->device_bytes() : 0;
+    return YB_OK;
+}
+
+yb_status yb_batch_gather(int32_t count, yb_sim* const* srcSims, const int32_t* srcScenes, yb_sim* recycle,
+                          int64_t capacityVerts, yb_sim** out) {
+    if (!out || count < 1 || !srcSims || !srcScenes) return YB_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    const int prec = srcSims[0] ? srcSims[0]->precision : -1;
+    std::vector<int32_t> counts(count);
+    long long total = 0;
+    for (int i = 0; i < count; i++) {
+        yb_sim* x = srcSims[i];
+        if (!x || x == recycle || x->precision != prec) return YB_ERR_INVALID_ARGUMENT;
+        if (!x->configured) return YB_ERR_NOT_CONFIGURED;
+        if (srcScenes[i] < 0 || srcScenes[i] >= x->numScenes) return YB_ERR_INVALID_ARGUMENT;
+        counts[i] = x->sceneOff[srcScenes[i] + 1] - x->sceneOff[srcScenes[i]];
+        total += counts[i];
+    }
+    if (total > (1LL << 31) / YB_MAX_COLLISIONS_PER_SEGMENT) return YB_ERR_INVALID_ARGUMENT;
+    yb_sim* S = nullptr;
+    if (recycle && recycle->configured && recycle->precision == prec && recycle->capVerts >= total &&
+        recycle->capScenes >= count) {
+        S = recycle;
+        cudaStreamSynchronize(S->stream);
+    } else {
+        const yb_status st = create_internal(count, counts.data(), prec, capacityVerts,
+                                             (int32_t)std::max<int64_t>(count, capacityVerts / 64), &S);
+        if (st != YB_OK) return st;
+    }
+    // host-side layout, parameters and host arrays follow the sources
+    S->n = (int)total;
+    S->numScenes = count;
+    S->sceneOff.assign(count + 1, 0);
+    S->meta.resize(count);
+    S->initialInvMasses.resize(total);
+    S->maxH = srcSims[0]->maxH;
+    for (int i = 0; i < count; i++) {
+        yb_sim* x = srcSims[i];
+        const int so = x->sceneOff[srcScenes[i]], m = counts[i];
+        const int to = S->sceneOff[i];
+        S->sceneOff[i + 1] = to + m;
+        S->meta[i] = x->meta[srcScenes[i]];
+        std::memcpy(S->verts + to, x->verts + so, sizeof(yb_vertex) * m);
+        std::memcpy(S->vels + 3 * (size_t)to, x->vels + 3 * (size_t)so, 12 * (size_t)m);
+        std::memcpy(S->qs + 4 * (size_t)to, x->qs + 4 * (size_t)so, 16 * (size_t)m);
+        std::memcpy(S->qRests + 4 * (size_t)to, x->qRests + 4 * (size_t)so, 16 * (size_t)m);
+        if ((int)x->initialInvMasses.size() >= so + m)
+            std::memcpy(S->initialInvMasses.data() + to, x->initialInvMasses.data() + so, sizeof(float) * m);
+        for (int v = to; v < to + m; v++)
+            if (S->verts[v].connectionIndex >= 0) S->verts[v].connectionIndex += to - so;
+    }
+    S->stepCounter = 0;
+    S->lastBVHRebuild = INFINITY;
+    S->iterThreads = srcSims[0]->iterThreads;
+    S->iterLanes = srcSims[0]->iterLanes;
+    S->iterPipe = srcSims[0]->iterPipe;
+    if (!S->configured) {
+        cudaError_t e = cudaStreamCreateWithFlags(&S->ownStream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            yb_destroy(S);
+            return cuda_status(e);
+        }
+        S->stream = S->ownStream;
+        S->eng = make_engine(S);
+        yb_status st = S->eng ? engine_alloc(S) : YB_ERR_OUT_OF_MEMORY;
+        if (st != YB_OK) {
+            yb_destroy(S);
+            return st;
+        }
+        S->configured = true;
+    }
+    yb_status st = S->eng->gather(count, srcSims, srcScenes);
+    if (st == YB_OK) st = validate_all_meta(S);
+    if (st == YB_OK) S->eng->write_params();
+    if (st != YB_OK) {
+        if (S != recycle) yb_destroy(S);
+        return st;
+    }
+    *out = S;
+    return YB_OK;
 }
 
 yb_status yb_launch_count(yb_sim* S, uint64_t* out) {

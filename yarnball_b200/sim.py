@@ -64,22 +64,39 @@ class Sim:
     ERROR_MAX_COLLISIONS_PER_SEGMENT_EXCEEDED = 1
     WARNING_SEGMENT_INTERPENETRATION = 2
 
-    def __init__(self, numVerts=None, *, scenes=None, precision="fp32"):
+    def __init__(self, numVerts=None, *, scenes=None, precision="fp32", _handle=None):
         """Sim(numVerts) as YarnBall.cu:11-51, or a batch of independent scenes
         (scenes = list of vertex counts).  precision: "fp32" or "fp64"."""
         self._lib = _abi.load()
-        self._h = ctypes.c_void_p()
-        prec = {"fp32": 0, "fp64": 1}[precision]
-        if scenes is None:
-            if numVerts is None:
-                raise ValueError("numVerts or scenes required")
-            scenes = [int(numVerts)]
-        counts = np.ascontiguousarray(np.asarray(scenes, dtype=np.int32))
-        check(self._lib.yb_create_batch(len(counts), ptr(counts, ctypes.c_int32), prec, ctypes.byref(self._h)), "Sim")
-        self.numScenes = len(counts)
-        self.sceneOffsets = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
-        self.numVerts = int(self.sceneOffsets[-1])
-        self.precision = precision
+        if _handle is not None:
+            self._h = _handle
+        else:
+            self._h = ctypes.c_void_p()
+            prec = {"fp32": 0, "fp64": 1}[precision]
+            if scenes is None:
+                if numVerts is None:
+                    raise ValueError("numVerts or scenes required")
+                scenes = [int(numVerts)]
+            counts = np.ascontiguousarray(np.asarray(scenes, dtype=np.int32))
+            check(self._lib.yb_create_batch(len(counts), ptr(counts, ctypes.c_int32), prec, ctypes.byref(self._h)),
+                  "Sim")
+        self._bind_views()
+        self.meta = _MetaView(self, 0)
+        self.printErrors = True
+
+    def _bind_views(self):
+        """(Re)creates the numpy views of the host arrays for the current layout."""
+        nv, ns, pr = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        check(self._lib.yb_info(self._h, ctypes.byref(nv), ctypes.byref(ns), ctypes.byref(pr)))
+        self.numScenes = ns.value
+        offs = [0]
+        for s in range(ns.value):
+            f, c = ctypes.c_int32(), ctypes.c_int32()
+            check(self._lib.yb_scene_range(self._h, s, ctypes.byref(f), ctypes.byref(c)))
+            offs.append(f.value + c.value)
+        self.sceneOffsets = np.array(offs, np.int64)
+        self.numVerts = nv.value
+        self.precision = "fp64" if pr.value == 1 else "fp32"
         vp = ctypes.c_void_p()
         qp, qrp, vlp = _abi.c_float_p(), _abi.c_float_p(), _abi.c_float_p()
         check(self._lib.yb_host_arrays(self._h, ctypes.byref(vp), ctypes.byref(qp), ctypes.byref(qrp),
@@ -90,8 +107,6 @@ class Sim:
         self.qs = np.ctypeslib.as_array(qp, shape=(n, 4))
         self.qRests = np.ctypeslib.as_array(qrp, shape=(n, 4))
         self.vels = np.ctypeslib.as_array(vlp, shape=(n, 3))
-        self.meta = _MetaView(self, 0)
-        self.printErrors = True
 
     # ---- lifecycle -------------------------------------------------------------------
     def close(self):
@@ -206,20 +221,47 @@ class Sim:
         return np.ctypeslib.as_array(p, shape=(c.value,)).copy()
 
     # ---- additions -------------------------------------------------------------------
-    def set_tuning(self, iterThreads=256, lanesPerVertex=4, useGraphs=True):
-        check(self._lib.yb_set_tuning(self._h, int(iterThreads), int(lanesPerVertex), 1 if useGraphs else 0),
-              "tuning")
+    def set_tuning(self, iterThreads=256, lanesPerVertex=4, useGraphs=True, pipelined=False):
+        check(self._lib.yb_set_tuning(self._h, int(iterThreads), int(lanesPerVertex), 1 if pipelined else 0,
+                                      1 if useGraphs else 0), "tuning")
 
     def get_tuning(self):
-        t, l, g = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
-        check(self._lib.yb_get_tuning(self._h, ctypes.byref(t), ctypes.byref(l), ctypes.byref(g)))
-        return t.value, l.value, bool(g.value)
+        t, l, p, g = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        check(self._lib.yb_get_tuning(self._h, ctypes.byref(t), ctypes.byref(l), ctypes.byref(p), ctypes.byref(g)))
+        return t.value, l.value, bool(p.value), bool(g.value)
 
     def autotune(self):
-        """Times every Newton-kernel shape on the current state and keeps the fastest."""
-        t, l, ms = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_float()
-        check(self._lib.yb_autotune(self._h, ctypes.byref(t), ctypes.byref(l), ctypes.byref(ms)), "autotune")
-        return t.value, l.value, ms.value
+        """Times every Newton-kernel shape on the current state and keeps the fastest:
+        returns (threads, lanes per vertex, pipelined, ms per launch)."""
+        t, l, p, ms = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32(), ctypes.c_float()
+        check(self._lib.yb_autotune(self._h, ctypes.byref(t), ctypes.byref(l), ctypes.byref(p), ctypes.byref(ms)),
+              "autotune")
+        return t.value, l.value, bool(p.value), ms.value
+
+    def download_scene(self, scene):
+        check(self._lib.yb_download_scene(self._h, int(scene)), "download_scene")
+
+    def device_bytes(self):
+        v = ctypes.c_uint64()
+        check(self._lib.yb_device_bytes(self._h, ctypes.byref(v)))
+        return int(v.value)
+
+    @staticmethod
+    def gather(sources, recycle=None, capacity=0):
+        """A batch made of copies of scenes (sim, scene) taken device to device; reuses the
+        device allocation of `recycle` (a batch) when it is large enough, else allocates room
+        for max(total, capacity) vertices."""
+        lib = _abi.load()
+        n = len(sources)
+        sims = (ctypes.c_void_p * n)(*[s._h.value for s, _ in sources])
+        idx = np.ascontiguousarray([int(k) for _, k in sources], dtype=np.int32)
+        out = ctypes.c_void_p()
+        rec = recycle._h if recycle is not None else None
+        check(lib.yb_batch_gather(n, sims, ptr(idx, ctypes.c_int32), rec, int(capacity), ctypes.byref(out)), "gather")
+        if recycle is not None and out.value == recycle._h.value:
+            recycle._bind_views()
+            return recycle
+        return Sim(_handle=out)
 
     def set_stream(self, stream_handle):
         """Launch on a caller's cudaStream_t (int handle, e.g. torch's stream.cuda_stream); 0 = own."""
