@@ -147,6 +147,25 @@ def test_dense_pile_substep_vs_fp64():
     assert qerr <= 1e-5, qerr
 
 
+SHAPES = [(256, 1, False), (128, 1, False), (256, 2, False), (256, 4, False), (512, 4, False), (256, 8, False),
+          (512, 8, False), (128, 1, True), (256, 1, True), (256, 4, True), (256, 0, False), (128, 0, False)]
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+def test_every_newton_kernel_shape_vs_fp64(shape):
+    """Each autotuner candidate (threads, lanes per vertex, pipelined; lanes 0 = balanced)
+    meets the one-substep tolerance on the contact-heavy dense pile."""
+    sim = scenes.build_pile(seed=9, yarns=96, verts=64, cube=0.03)
+    sim.set_tuning(shape[0], shape[1], True, shape[2])
+    orc = oracle.from_sim(sim, mode=oracle.FP64)
+    sim.advance(1e-3)
+    orc.advance(1e-3, 1e-3)
+    pos, _, q = sim.read_state_f64()
+    ref = orc.state()
+    assert np.abs(pos - ref["pos"]).max() <= 1e-5 * SEG
+    assert quat_angle(q[seg_rows(sim)], ref["q"][seg_rows(sim)]).max() <= 1e-5
+
+
 def test_batched_equals_alone():
     spec = scenes.batched_spec(seed=5, num_scenes=5, cap=200000, max_yarns=12, min_len=32, max_len=400)
     assert len(spec[0]) == 5
