@@ -9,7 +9,7 @@
 //   * advance() returns dt (the reference declares float but returns nothing);
 //   * when <glm/glm.hpp> is available vec3/vec4 are glm's, otherwise minimal POD structs
 //     with the same layout; Rotor is a POD {x, y, z, w} (w scalar), like Kit::Rotor's layout;
-//   * rendering, file export and the fibre mesher are not part of this library.
+//   * rendering and the fibre mesher are not part of this library.
 #pragma once
 #include <cstdint>
 #include <cstdio>
@@ -202,6 +202,17 @@ class Sim {
         printf("Segments with collisions: %d/%d\n", segs, meta.numVerts);
     }
 
+    // io/fileExport.cpp:6-100.  Like the reference, a path that cannot be opened prints
+    // "Error opening file" and returns.
+    void exportToBCC(std::string path, bool exportAsPolyline = false) {
+        push();
+        report_file(yb_export_bcc(h_, path.c_str(), exportAsPolyline ? 1 : 0));
+    }
+    void exportToOBJ(std::string path) {
+        push();
+        report_file(yb_export_obj(h_, path.c_str()));
+    }
+
     yb_sim* handle() { return h_; }
 
    private:
@@ -209,6 +220,13 @@ class Sim {
 
     static void check(yb_status st) {
         if (st != YB_OK) throw std::runtime_error(yb_status_string(st));
+    }
+    static void report_file(yb_status st) {
+        if (st == YB_ERR_INVALID_ARGUMENT) {
+            fprintf(stdout, "Error opening file\n");
+            return;
+        }
+        check(st);
     }
     void push() {
         check(yb_set_meta(h_, 0, reinterpret_cast<const yb_meta*>(&meta)));

@@ -216,6 +216,45 @@ yb_status yb_batch_gather(int32_t count, yb_sim* const* srcSims, const int32_t* 
 /* download() restricted to one scene of a batch (its range of the host arrays). */
 yb_status yb_download_scene(yb_sim* sim, int32_t scene);
 
+/* Kinematic driver for pinned vertices, on the device.  It performs the reference's
+ * per-frame twist and pull scenarios (KittenEngine/main.cpp:54-121: download, move the pinned
+ * vertices, set their velocity, upload) without the host round trip.  group[v] = 0 leaves
+ * vertex v alone; g in 1..numMotions makes it follow motions[g-1] from its current position
+ * x0:  x(t) = c + Rot(axis, omega s) (x0 - c) + velocity s,  s = clamp(t - tStart, 0, tEnd - tStart),
+ * t being its scene's simulated time.  At the start of every advance(dt) each driven vertex is
+ * placed at x(t) with velocity (x(t+dt) - x(t)) / dt.  Driven vertices are normally pinned
+ * (invMass 0).  group = NULL switches the driver off. */
+typedef struct yb_pin_motion {
+    float center[3];
+    float axis[3];
+    float omega;
+    float velocity[3];
+    float tStart;
+    float tEnd;
+} yb_pin_motion;
+yb_status yb_set_pin_motion(yb_sim* sim, const uint8_t* group, int32_t numMotions, const yb_pin_motion* motions);
+
+/* Sim::exportToBCC (io/fileExport.cpp:6-63): download(), then a 64-byte BCC header ('BCC',
+ * 0x44, curve type "PL" when asPolyline else "C0", 3 dimensions, up axis 1, curve and control
+ * point counts, 40 zero bytes) and each curve (a run of vertices with hasNext plus the vertex
+ * that ends it) as an int32 point count followed by float32 xyz per point.  Every scene of a
+ * batch is written into the one file.  An unopenable path gives YB_ERR_INVALID_ARGUMENT where
+ * the reference prints "Error opening file" and returns. */
+yb_status yb_export_bcc(yb_sim* sim, const char* path, int32_t asPolyline);
+
+/* Sim::exportToOBJ (io/fileExport.cpp:65-100): download(), then "v x y z" lines with 16
+ * decimals and one "l i j ..." polyline (1-based) per curve. */
+yb_status yb_export_obj(yb_sim* sim, const char* path);
+
+/* Full-state checkpoint (no reference counterpart; the exporters above keep positions only).
+ * Writes the device state in the simulation's precision (positions with their compensation
+ * terms, velocities, last velocities, rotors, rest rotors, per-vertex constants, the contact
+ * lists), every scene's meta, maxH, the step counter and the Newton kernel shape.  A
+ * simulation restored by yb_load_state continues bit-identically to one that never stopped.
+ * Pin motions (yb_set_pin_motion) are not saved.  Requires a configured simulation. */
+yb_status yb_save_state(yb_sim* sim, const char* path);
+yb_status yb_load_state(const char* path, yb_sim** out);
+
 /* First vertex and vertex count of a scene. */
 yb_status yb_scene_range(yb_sim* sim, int32_t scene, int32_t* first, int32_t* count);
 

@@ -76,6 +76,11 @@ class YbMeta(ctypes.Structure):
     ]
 
 
+class YbPinMotion(ctypes.Structure):
+    _fields_ = [("center", ctypes.c_float * 3), ("axis", ctypes.c_float * 3), ("omega", ctypes.c_float),
+                ("velocity", ctypes.c_float * 3), ("tStart", ctypes.c_float), ("tEnd", ctypes.c_float)]
+
+
 # name -> (restype, argtypes)
 _P = ctypes.c_void_p
 SIGNATURES = {
@@ -111,6 +116,12 @@ SIGNATURES = {
     "yb_download_scene": (ctypes.c_int, [_P, ctypes.c_int32]),
     "yb_device_bytes": (ctypes.c_int, [_P, c_uint64_p]),
     "yb_scene_range": (ctypes.c_int, [_P, ctypes.c_int32, c_int32_p, c_int32_p]),
+    "yb_export_bcc": (ctypes.c_int, [_P, ctypes.c_char_p, ctypes.c_int32]),
+    "yb_export_obj": (ctypes.c_int, [_P, ctypes.c_char_p]),
+    "yb_save_state": (ctypes.c_int, [_P, ctypes.c_char_p]),
+    "yb_load_state": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_P)]),
+    "yb_set_pin_motion": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint8), ctypes.c_int32,
+                                         ctypes.POINTER(YbPinMotion)]),
     "yb_set_stream": (ctypes.c_int, [_P, _P]),
     "yb_profile_advance": (ctypes.c_int, [_P, ctypes.c_float, c_double_p, c_uint64_p]),
     "yb_info": (ctypes.c_int, [_P, c_int32_p, c_int32_p, c_int32_p]),

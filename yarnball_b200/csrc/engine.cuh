@@ -79,6 +79,15 @@ struct SceneParams {
     R sdr;                          // scaledDetectionRadius
     R stepBase;                     // detectionRadius * (detectionScaler - 1)
     int useStepLimit, useVelRadius;
+    double time;                    // simulated time at the start of the current advance()
+};
+
+// Prescribed rigid motion of a group of pinned vertices (see yb_set_pin_motion).
+struct PinMotion {
+    double c[3], a[3];  // rotation centre and unit axis
+    double omega;       // rad/s
+    double v[3];        // translation velocity
+    double t0, t1;      // motion active for simulated time in [t0, t1]
 };
 
 template <typename R>
@@ -128,7 +137,11 @@ template <typename R> void launch_bvh_rebuild(const Dev<R>& d, cudaStream_t s, v
 template <typename R> void launch_bvh_refit(const Dev<R>& d, cudaStream_t s);
 template <typename R> void launch_traverse(const Dev<R>& d, cudaStream_t s);  // + list sort + step limit (2 kernels)
 template <typename R> void launch_lists_step_limit(const Dev<R>& d, cudaStream_t s);  // step limit over segments
-template <typename R> void launch_bvh_reset(const Dev<R>& d, cudaStream_t s);  // scene roots := empty
+template <typename R> void launch_bvh_reset(const Dev<R>& d, cudaStream_t s);
+// Places driven vertices on their prescribed motion at the start of an advance of length dt.
+template <typename R>
+void launch_pin_drive(const Dev<R>& d, const float4* init, const unsigned char* group, const PinMotion* m, double dt,
+                      cudaStream_t s);  // scene roots := empty
 
 // Radix sort of (u64 key, int value) pairs, ascending by the low `bits` key bits, stable.
 // keys/vals ping-pong between [0] and [1]; the result lands in buffer (passes & 1).

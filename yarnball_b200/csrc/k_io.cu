@@ -79,6 +79,43 @@ __global__ void k_relayout(Dev<R> d, const int* __restrict__ sceneOf, const int*
     d.vp[i] = vp;
 }
 
+// Kinematic driver (the per-frame twist/pull of KittenEngine/main.cpp:54-121, on the device):
+// x(t) = c + Rot(a, omega s(t)) (x0 - c) + v s(t), s(t) = clamp(t - t0, 0, t1 - t0).
+__device__ inline void pin_place(const PinMotion& m, const double x0[3], double t, double out[3]) {
+    const double s = fmin(fmax(t - m.t0, 0.0), m.t1 - m.t0);
+    const double th = m.omega * s;
+    const double ct = cos(th), st = sin(th);
+    const double r[3] = {x0[0] - m.c[0], x0[1] - m.c[1], x0[2] - m.c[2]};
+    const double kd = m.a[0] * r[0] + m.a[1] * r[1] + m.a[2] * r[2];
+    const double kx[3] = {m.a[1] * r[2] - m.a[2] * r[1], m.a[2] * r[0] - m.a[0] * r[2], m.a[0] * r[1] - m.a[1] * r[0]};
+    for (int i = 0; i < 3; i++)
+        out[i] = m.c[i] + r[i] * ct + kx[i] * st + m.a[i] * kd * (1.0 - ct) + m.v[i] * s;
+}
+
+template <typename R>
+__global__ void k_pin_drive(Dev<R> d, const float4* __restrict__ init, const unsigned char* __restrict__ group,
+                            const PinMotion* __restrict__ motions, double dt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.n) return;
+    const int g = group[i];
+    if (g == 0) return;
+    const PinMotion& m = motions[g - 1];
+    const double t = d.sp[scene_of(d.vp[i].flags)].time;
+    const float4 x0f = init[i];
+    const double x0[3] = {x0f.x, x0f.y, x0f.z};
+    double a[3], b[3];
+    pin_place(m, x0, t, a);
+    pin_place(m, x0, t + dt, b);
+    V4<R> p = d.pos[i];
+    p.x = (R)a[0]; p.y = (R)a[1]; p.z = (R)a[2];
+    d.pos[i] = p;
+    V4<R> z; z.x = R(0); z.y = R(0); z.z = R(0); z.w = R(0);
+    d.posC[i] = z;
+    V4<R> v;
+    v.x = (R)((b[0] - a[0]) / dt); v.y = (R)((b[1] - a[1]) / dt); v.z = (R)((b[2] - a[2]) / dt); v.w = R(0);
+    d.vel[i] = v;
+}
+
 template <typename R>
 __global__ void k_zero_vel(Dev<R> d) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -214,6 +251,12 @@ void launch_convert_out(const Dev<R>& d, void* hv, float* hvel, float* hq, int f
     k_convert_out<R><<<(count + 255) / 256, 256, 0, s>>>(d, (HostVertex*)hv, hvel, hq, first, count);
 }
 template <typename R>
+void launch_pin_drive(const Dev<R>& d, const float4* init, const unsigned char* group, const PinMotion* m, double dt,
+                      cudaStream_t s) {
+    if (d.n <= 0) return;
+    k_pin_drive<R><<<(d.n + 255) / 256, 256, 0, s>>>(d, init, group, m, dt);
+}
+template <typename R>
 void launch_relayout(const Dev<R>& d, const int* sceneOf, const int* delta, cudaStream_t s) {
     if (d.n <= 0) return;
     k_relayout<R><<<(d.n + 255) / 256, 256, 0, s>>>(d, sceneOf, delta);
@@ -244,6 +287,8 @@ int launch_diag(const Dev<R>& d, double* part, cudaStream_t s) {
                                        const int*, cudaStream_t);                                            \
     template void launch_convert_out<R>(const Dev<R>&, void*, float*, float*, int, int, cudaStream_t);       \
     template void launch_relayout<R>(const Dev<R>&, const int*, const int*, cudaStream_t);                   \
+    template void launch_pin_drive<R>(const Dev<R>&, const float4*, const unsigned char*, const PinMotion*, double, \
+                                      cudaStream_t);                                                         \
     template void launch_zero_vel<R>(const Dev<R>&, cudaStream_t);                                           \
     template void launch_state_f64<R>(const Dev<R>&, int, double*, double*, double*, double*, cudaStream_t); \
     template void launch_scene_root_box<R>(const Dev<R>&, float*, cudaStream_t);                             \

@@ -18,6 +18,7 @@
 // once as a CUDA graph and replayed.
 #include <cmath>
 #include <cfloat>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <new>
@@ -54,6 +55,10 @@ struct EngineBase {
     virtual yb_status download_range(int first, int count) = 0;
     virtual yb_status gather(int count, yb_sim* const* src, const int* srcScenes) = 0;
     virtual size_t device_bytes() const = 0;
+    virtual yb_status set_pins(const unsigned char* group, int numMotions, const PinMotion* motions) = 0;
+    virtual yb_status save_device(FILE* f) = 0;
+    virtual yb_status load_device(FILE* f) = 0;
+    virtual yb_status drive_pins(double dt) = 0;
 };
 
 }  // namespace
@@ -266,6 +271,7 @@ SceneParams<R> scene_params_of(const yb_meta& m) {
     p.stepBase = dr * ((R)m.detectionScaler - R(1));
     p.useStepLimit = m.useStepSizeLimit ? 1 : 0;
     p.useVelRadius = m.useVelocityRadius ? 1 : 0;
+    p.time = m.time;
     return p;
 }
 
@@ -302,6 +308,7 @@ struct Engine : EngineBase {
         for (auto& g : graphs)
             if (g) cudaGraphExecDestroy(g);
         if (block) cudaFree(block);
+        if (pinMem) cudaFree(pinMem);
         if (spHost) cudaFreeHost(spHost);
         if (errHost) cudaFreeHost(errHost);
     }
@@ -388,6 +395,95 @@ struct Engine : EngineBase {
     }
 
     size_t device_bytes() const override { return allocBytes; }
+
+    // Kinematic pin driver state (allocated on first use).
+    void* pinMem = nullptr;
+    float4* pinInit = nullptr;
+    unsigned char* pinGroup = nullptr;
+    PinMotion* pinMotion = nullptr;
+    bool pinsOn = false;
+
+    yb_status set_pins(const unsigned char* group, int numMotions, const PinMotion* motions) override {
+        if (!group) {
+            pinsOn = false;
+            return YB_OK;
+        }
+        const size_t cap = (size_t)S->capVerts;
+        if (!pinMem) {
+            const size_t bytes = (sizeof(float4) * cap + 255) / 256 * 256 + (cap + 255) / 256 * 256 +
+                                 sizeof(PinMotion) * 255;
+            YB_CUDA(cudaMalloc(&pinMem, bytes));
+            pinInit = (float4*)pinMem;
+            pinGroup = (unsigned char*)pinMem + (sizeof(float4) * cap + 255) / 256 * 256;
+            pinMotion = (PinMotion*)(pinGroup + (cap + 255) / 256 * 256);
+        }
+        const size_t n = (size_t)S->n;
+        cudaStream_t st = S->stream;
+        // reference positions: the current device positions
+        std::vector<double> pos(3 * n);
+        YB_CUDA(read_state_f64(pos.data(), nullptr, nullptr, nullptr, 0) == YB_OK ? cudaSuccess : cudaErrorUnknown);
+        std::vector<float4> init(n);
+        for (size_t i = 0; i < n; i++) init[i] = make_float4((float)pos[3 * i], (float)pos[3 * i + 1], (float)pos[3 * i + 2], 0.f);
+        YB_CUDA(cudaMemcpyAsync(pinInit, init.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, st));
+        YB_CUDA(cudaMemcpyAsync(pinGroup, group, n, cudaMemcpyHostToDevice, st));
+        YB_CUDA(cudaMemcpyAsync(pinMotion, motions, sizeof(PinMotion) * numMotions, cudaMemcpyHostToDevice, st));
+        YB_CUDA(cudaStreamSynchronize(st));
+        pinsOn = true;
+        return YB_OK;
+    }
+
+    // Checkpoint: the device state in the simulation's precision, in a fixed order, then the
+    // contact lists (kept across substeps without detection when detectionPeriod > 1).
+    std::vector<std::pair<void*, size_t>> state_arrays() {
+        const size_t n = (size_t)S->n;
+        return {{d.pos, sizeof(V4<R>) * n},     {d.posC, sizeof(V4<R>) * n}, {d.vel, sizeof(V4<R>) * n},
+                {d.lastVel, sizeof(V4<R>) * n}, {d.q[0], sizeof(V4<R>) * n}, {d.qRest, sizeof(V4<R>) * n},
+                {d.vp, sizeof(VP<R>) * n},      {d.numCols, sizeof(int) * n}};
+    }
+
+    yb_status save_device(FILE* f) override {
+        YB_CUDA(cudaStreamSynchronize(S->stream));
+        int32_t maxNc = 0;
+        for (auto& a : state_arrays()) {
+            std::vector<char> h(a.second);
+            YB_CUDA(cudaMemcpy(h.data(), a.first, a.second, cudaMemcpyDeviceToHost));
+            if (a.first == (void*)d.numCols)
+                for (int i = 0; i < S->n; i++) maxNc = std::max(maxNc, ((const int32_t*)h.data())[i]);
+            if (fwrite(h.data(), 1, a.second, f) != a.second) return YB_ERR_INVALID_ARGUMENT;
+        }
+        // cols is column major [k + n * c]: the first maxNc columns hold every listed contact.
+        const size_t colBytes = sizeof(int) * (size_t)S->n * (size_t)maxNc;
+        std::vector<char> h(colBytes);
+        if (colBytes) YB_CUDA(cudaMemcpy(h.data(), d.cols, colBytes, cudaMemcpyDeviceToHost));
+        if (fwrite(&maxNc, 4, 1, f) != 1 || fwrite(h.data(), 1, colBytes, f) != colBytes) return YB_ERR_INVALID_ARGUMENT;
+        return YB_OK;
+    }
+
+    yb_status load_device(FILE* f) override {
+        for (auto& a : state_arrays()) {
+            std::vector<char> h(a.second);
+            if (fread(h.data(), 1, a.second, f) != a.second) return YB_ERR_INVALID_ARGUMENT;
+            YB_CUDA(cudaMemcpy(a.first, h.data(), a.second, cudaMemcpyHostToDevice));
+        }
+        int32_t maxNc = -1;
+        if (fread(&maxNc, 4, 1, f) != 1 || maxNc < 0 || maxNc > MAX_COLS) return YB_ERR_INVALID_ARGUMENT;
+        const size_t colBytes = sizeof(int) * (size_t)S->n * (size_t)maxNc;
+        std::vector<char> h(colBytes);
+        if (fread(h.data(), 1, colBytes, f) != colBytes) return YB_ERR_INVALID_ARGUMENT;
+        if (colBytes) YB_CUDA(cudaMemcpy(d.cols, h.data(), colBytes, cudaMemcpyHostToDevice));
+        // Host arrays and the segment list from the restored state (not convert_in, which
+        // would reset the compensation terms); the BVH is rebuilt by the next detection.
+        const yb_status st = download();
+        return st == YB_OK ? refresh_segments() : st;
+    }
+
+    yb_status drive_pins(double dt) override {
+        if (!pinsOn) return YB_OK;
+        launch_pin_drive(d, pinInit, pinGroup, pinMotion, dt, S->stream);
+        S->launches++;
+        YB_CUDA(cudaGetLastError());
+        return YB_OK;
+    }
 
     // Segment list from the host flags (the rule of upload()).
     yb_status refresh_segments() {
@@ -1016,6 +1112,8 @@ yb_status yb_advance(yb_sim* S, float dt, float* advanced) {
     yb_status st = validate_all_meta(S);
     if (st != YB_OK) return st;
     S->eng->write_params();
+    st = S->eng->drive_pins(dt);
+    if (st != YB_OK) return st;
     const yb_meta& m0 = S->meta[0];
     for (int s = 0; s < steps; s++, S->stepCounter++) {
         int type = 2;
@@ -1211,6 +1309,177 @@ yb_status yb_download_scene(yb_sim* S, int32_t scene) {
     if (!S || scene < 0 || scene >= S->numScenes) return YB_ERR_INVALID_ARGUMENT;
     if (!S->configured) return YB_ERR_NOT_CONFIGURED;
     return S->eng->download_range(S->sceneOff[scene], S->sceneOff[scene + 1] - S->sceneOff[scene]);
+}
+
+yb_status yb_set_pin_motion(yb_sim* S, const uint8_t* group, int32_t numMotions, const yb_pin_motion* motions) {
+    if (!S || (group && (numMotions < 1 || numMotions > 255 || !motions))) return YB_ERR_INVALID_ARGUMENT;
+    if (!S->configured) return YB_ERR_NOT_CONFIGURED;
+    std::vector<PinMotion> m(group ? numMotions : 0);
+    for (size_t g = 0; g < m.size(); g++) {
+        const yb_pin_motion& x = motions[g];
+        double a[3] = {x.axis[0], x.axis[1], x.axis[2]};
+        const double l = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+        if (!(l > 0) && x.omega != 0.f) return YB_ERR_INVALID_ARGUMENT;
+        for (int i = 0; i < 3; i++) {
+            m[g].c[i] = x.center[i];
+            m[g].a[i] = l > 0 ? a[i] / l : 0.0;
+            m[g].v[i] = x.velocity[i];
+        }
+        m[g].omega = x.omega;
+        m[g].t0 = x.tStart;
+        m[g].t1 = x.tEnd;
+    }
+    if (group)
+        for (int i = 0; i < S->n; i++)
+            if (group[i] > numMotions) return YB_ERR_INVALID_ARGUMENT;
+    return S->eng->set_pins(group, (int)m.size(), m.data());
+}
+
+// ---- files: BCC / OBJ export (fileExport.cpp:6-100) and full-state checkpoints ----------
+
+// Runs of consecutive segment vertices [start, end] (end = the first vertex without hasNext).
+static std::vector<std::pair<int, int>> curve_runs(const yb_sim* S) {
+    std::vector<std::pair<int, int>> runs;
+    bool last = false;
+    int start = 0;
+    for (int i = 0; i < S->n; i++) {
+        const bool seg = (S->verts[i].flags & YB_HAS_NEXT) != 0;
+        if (seg && !last) start = i;
+        if (!seg && last) runs.push_back({start, i});
+        last = seg;
+    }
+    return runs;
+}
+
+yb_status yb_export_bcc(yb_sim* S, const char* path, int32_t asPolyline) {
+    if (!S || !path) return YB_ERR_INVALID_ARGUMENT;
+    yb_status st = yb_download(S);
+    if (st != YB_OK) return st;
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return YB_ERR_INVALID_ARGUMENT;
+    unsigned char hdr[64];
+    std::memset(hdr, 0, sizeof(hdr));
+    hdr[0] = 'B'; hdr[1] = 'C'; hdr[2] = 'C';
+    hdr[3] = 0x44;
+    hdr[4] = asPolyline ? 'P' : 'C';
+    hdr[5] = asPolyline ? 'L' : '0';
+    hdr[6] = 3;  // dimensions
+    hdr[7] = 1;  // up dimension
+    const auto runs = curve_runs(S);
+    uint64_t curves = runs.size(), points = 0;
+    for (auto& r : runs) points += (uint64_t)(r.second - r.first + 1);
+    std::memcpy(hdr + 8, &curves, 8);
+    std::memcpy(hdr + 16, &points, 8);
+    bool ok = std::fwrite(hdr, 1, 64, f) == 64;
+    for (auto& r : runs) {
+        const int32_t np = r.second - r.first + 1;
+        ok = ok && std::fwrite(&np, 4, 1, f) == 1;
+        for (int i = r.first; i <= r.second; i++) ok = ok && std::fwrite(S->verts[i].pos, 4, 3, f) == 3;
+    }
+    std::fclose(f);
+    return ok ? YB_OK : YB_ERR_INVALID_ARGUMENT;
+}
+
+yb_status yb_export_obj(yb_sim* S, const char* path) {
+    if (!S || !path) return YB_ERR_INVALID_ARGUMENT;
+    yb_status st = yb_download(S);
+    if (st != YB_OK) return st;
+    FILE* f = std::fopen(path, "w");
+    if (!f) return YB_ERR_INVALID_ARGUMENT;
+    std::fprintf(f, "# YarnBall Sim\n\no YarnBall\n\n# Vertices (in meters)\n");
+    for (int i = 0; i < S->n; i++)
+        std::fprintf(f, "v %.16f %.16f %.16f\n", S->verts[i].pos[0], S->verts[i].pos[1], S->verts[i].pos[2]);
+    std::fprintf(f, "\n# Curves\n");
+    bool last = false;
+    for (int i = 0; i < S->n; i++) {
+        const bool seg = (S->verts[i].flags & YB_HAS_NEXT) != 0;
+        if (seg) {
+            if (!last) std::fprintf(f, "l %d", i + 1);
+            std::fprintf(f, " %d", i + 2);
+        } else if (last) {
+            std::fprintf(f, "\n");
+        }
+        last = seg;
+    }
+    std::fclose(f);
+    return YB_OK;
+}
+
+static const char CKPT_MAGIC[8] = {'Y', 'B', 'C', 'K', 'P', 'T', '0', '1'};
+
+yb_status yb_save_state(yb_sim* S, const char* path) {
+    if (!S || !path) return YB_ERR_INVALID_ARGUMENT;
+    if (!S->configured) return YB_ERR_NOT_CONFIGURED;
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return YB_ERR_INVALID_ARGUMENT;
+    bool ok = std::fwrite(CKPT_MAGIC, 1, 8, f) == 8;
+    const int32_t hdr[3] = {S->precision, S->n, S->numScenes};
+    ok = ok && std::fwrite(hdr, 4, 3, f) == 3;
+    std::vector<int32_t> counts(S->numScenes);
+    for (int s = 0; s < S->numScenes; s++) counts[s] = S->sceneOff[s + 1] - S->sceneOff[s];
+    ok = ok && std::fwrite(counts.data(), 4, counts.size(), f) == counts.size();
+    ok = ok && std::fwrite(S->meta.data(), sizeof(yb_meta), S->meta.size(), f) == S->meta.size();
+    ok = ok && std::fwrite(&S->maxH, 4, 1, f) == 1;
+    ok = ok && std::fwrite(&S->stepCounter, 8, 1, f) == 1;
+    ok = ok && std::fwrite(&S->lastBVHRebuild, 4, 1, f) == 1;
+    const int32_t tune[4] = {S->iterThreads, S->iterLanes, S->iterPipe, S->useGraphs};
+    ok = ok && std::fwrite(tune, 4, 4, f) == 4;
+    ok = ok && std::fwrite(S->qRests, 16, S->n, f) == (size_t)S->n;
+    ok = ok && std::fwrite(S->initialInvMasses.data(), 4, S->initialInvMasses.size(), f) == S->initialInvMasses.size();
+    yb_status st = ok ? S->eng->save_device(f) : YB_ERR_INVALID_ARGUMENT;
+    std::fclose(f);
+    return st;
+}
+
+yb_status yb_load_state(const char* path, yb_sim** out) {
+    if (!path || !out) return YB_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return YB_ERR_INVALID_ARGUMENT;
+    char magic[8];
+    int32_t hdr[3];
+    bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, CKPT_MAGIC, 8) == 0 &&
+              std::fread(hdr, 4, 3, f) == 3 && hdr[1] > 0 && hdr[2] > 0;
+    std::vector<int32_t> counts(ok ? hdr[2] : 0);
+    ok = ok && std::fread(counts.data(), 4, counts.size(), f) == counts.size();
+    yb_sim* S = nullptr;
+    yb_status st = ok ? create_internal(hdr[2], counts.data(), hdr[0], 0, 0, &S) : YB_ERR_INVALID_ARGUMENT;
+    if (st != YB_OK) {
+        std::fclose(f);
+        return st;
+    }
+    ok = std::fread(S->meta.data(), sizeof(yb_meta), S->meta.size(), f) == S->meta.size();
+    ok = ok && std::fread(&S->maxH, 4, 1, f) == 1 && std::fread(&S->stepCounter, 8, 1, f) == 1 &&
+         std::fread(&S->lastBVHRebuild, 4, 1, f) == 1;
+    int32_t tune[4] = {256, 4, 0, 1};
+    ok = ok && std::fread(tune, 4, 4, f) == 4;
+    S->iterThreads = tune[0]; S->iterLanes = tune[1]; S->iterPipe = tune[2]; S->useGraphs = tune[3];
+    ok = ok && std::fread(S->qRests, 16, S->n, f) == (size_t)S->n;
+    S->initialInvMasses.resize(S->n);
+    ok = ok && std::fread(S->initialInvMasses.data(), 4, S->n, f) == (size_t)S->n;
+    if (ok) {
+        cudaError_t e = cudaStreamCreateWithFlags(&S->ownStream, cudaStreamNonBlocking);
+        st = cuda_status(e);
+        if (st == YB_OK) {
+            S->stream = S->ownStream;
+            S->eng = make_engine(S);
+            st = S->eng ? engine_alloc(S) : YB_ERR_OUT_OF_MEMORY;
+        }
+        if (st == YB_OK) {
+            S->configured = true;
+            st = S->eng->load_device(f);
+        }
+    } else {
+        st = YB_ERR_INVALID_ARGUMENT;
+    }
+    std::fclose(f);
+    if (st == YB_OK) S->eng->write_params();
+    if (st != YB_OK) {
+        yb_destroy(S);
+        return st;
+    }
+    *out = S;
+    return YB_OK;
 }
 
 yb_status yb_scene_range(yb_sim* S, int32_t scene, int32_t* first, int32_t* count) {

@@ -181,6 +181,19 @@ class TwistDriver:
         self.t += dt
 
 
+def device_twist(sim, omega=2 * math.pi, t_start=0.0, t_end=1e30):
+    """Same motion as TwistDriver, performed on the device by the kinematic pin driver:
+    pinned vertices in the upper half rotate about the bundle axis (+y through the centre)."""
+    sim.download()
+    p = sim.verts["pos"].astype(np.float64)
+    ymax = p[:, 1].max()
+    top = (sim.verts["invMass"] == 0) & (p[:, 1] > 0.5 * ymax)
+    center = 0.5 * (p.min(0) + p.max(0))
+    groups = np.where(top, 1, 0).astype(np.uint8)
+    sim.set_pin_motion(groups, [dict(center=center, axis=(0, 1, 0), omega=omega, tStart=t_start, tEnd=t_end)])
+    return groups, center
+
+
 def batched_spec(seed=7, num_scenes=512, cap=8388608, max_yarns=64, min_len=64, max_len=4096):
     """Scene sizes of the batched workload: k ~ U{1..max_yarns} yarns per scene, vertices per
     yarn log-uniform in [min_len, max_len], kBend log-uniform in [1e-9, 1e-7]; scenes are

@@ -7,6 +7,7 @@ where the reference throws std::runtime_error.  All computation happens in the C
 behind the C ABI.
 """
 import ctypes
+import os
 
 import numpy as np
 
@@ -237,6 +238,43 @@ class Sim:
         check(self._lib.yb_autotune(self._h, ctypes.byref(t), ctypes.byref(l), ctypes.byref(p), ctypes.byref(ms)),
               "autotune")
         return t.value, l.value, bool(p.value), ms.value
+
+    def set_pin_motion(self, groups, motions):
+        """Device-side kinematic driver: groups (uint8 per vertex, 0 = free) select one of the
+        motions (dicts with center, axis, omega, velocity, tStart, tEnd); None switches it off."""
+        if groups is None:
+            check(self._lib.yb_set_pin_motion(self._h, None, 0, None), "set_pin_motion")
+            return
+        g = np.ascontiguousarray(groups, dtype=np.uint8)
+        arr = (_abi.YbPinMotion * len(motions))()
+        for i, m in enumerate(motions):
+            arr[i].center[:] = list(m.get("center", (0, 0, 0)))
+            arr[i].axis[:] = list(m.get("axis", (0, 1, 0)))
+            arr[i].omega = m.get("omega", 0.0)
+            arr[i].velocity[:] = list(m.get("velocity", (0, 0, 0)))
+            arr[i].tStart = m.get("tStart", 0.0)
+            arr[i].tEnd = m.get("tEnd", 1e30)
+        check(self._lib.yb_set_pin_motion(self._h, ptr(g, ctypes.c_uint8), len(motions), arr), "set_pin_motion")
+
+    # ---- files ------------------------------------------------------------------------
+    def exportToBCC(self, path, exportAsPolyline=False):
+        """Sim::exportToBCC (io/fileExport.cpp:6-63): downloads, then writes every curve."""
+        check(self._lib.yb_export_bcc(self._h, os.fsencode(path), int(bool(exportAsPolyline))), "exportToBCC")
+
+    def exportToOBJ(self, path):
+        """Sim::exportToOBJ (io/fileExport.cpp:65-100)."""
+        check(self._lib.yb_export_obj(self._h, os.fsencode(path)), "exportToOBJ")
+
+    def save_state(self, path):
+        """Full-state checkpoint; Sim.load_state(path) continues bit-identically."""
+        check(self._lib.yb_save_state(self._h, os.fsencode(path)), "save_state")
+
+    @staticmethod
+    def load_state(path):
+        lib = _abi.load()
+        out = ctypes.c_void_p()
+        check(lib.yb_load_state(os.fsencode(path), ctypes.byref(out)), "load_state")
+        return Sim(_handle=out)
 
     def download_scene(self, scene):
         check(self._lib.yb_download_scene(self._h, int(scene)), "download_scene")
