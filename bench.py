@@ -50,6 +50,7 @@ def parse():
     p.add_argument("--no-plain", action="store_true", help="skip the plain per-scene advance() loop")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     p.add_argument("--cap", type=int, default=8388608, help="vertex cap of the batched workload")
+    p.add_argument("--shape", default="", help="fixed Newton kernel shape threads,lanes,pipelined (default: autotune)")
     p.add_argument("--workload", default="batched", choices=["batched", "serve"])
     p.add_argument("--rate", type=float, default=4.0, help="serve: Poisson arrival rate (requests/s)")
     p.add_argument("--duration", type=float, default=10.0, help="serve: arrival window (s)")
@@ -246,8 +247,14 @@ def run_ours(args):
     sim.set_stream(stream.cuda_stream)
     for _ in range(args.warmup):
         sim.advance(FRAME)
-    # Autotuner: Newton-kernel shape (threads per block, lanes per vertex) timed on this state.
-    tune_threads, tune_lanes, tune_pipe, tune_ms = sim.autotune()
+    if args.shape:
+        # A fixed Newton-kernel shape "threads,lanes,pipelined" (lanes 0 = balanced kernel).
+        tune_threads, tune_lanes, tune_pipe = [int(x) for x in args.shape.split(",")]
+        sim.set_tuning(tune_threads, tune_lanes, True, bool(tune_pipe))
+        tune_ms = None
+    else:
+        # Autotuner: Newton-kernel shape (threads per block, lanes per vertex) timed on this state.
+        tune_threads, tune_lanes, tune_pipe, tune_ms = sim.autotune()
     cfg["newton_kernel_shape"] = {"threads": tune_threads, "lanes_per_vertex": tune_lanes, "pipelined": tune_pipe,
                                   "autotune_ms_per_launch": tune_ms}
     try:

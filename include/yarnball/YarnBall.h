@@ -9,7 +9,8 @@
 //   * advance() returns dt (the reference declares float but returns nothing);
 //   * when <glm/glm.hpp> is available vec3/vec4 are glm's, otherwise minimal POD structs
 //     with the same layout; Rotor is a POD {x, y, z, w} (w scalar), like Kit::Rotor's layout;
-//   * rendering and the fibre mesher are not part of this library.
+//   * rendering and the fibre mesher are not part of this library; the file readers and
+//     buildFromJSON are free functions here, as in the reference (YarnBall.h:208-211).
 #pragma once
 #include <cstdint>
 #include <cstdio>
@@ -24,6 +25,8 @@
 namespace YarnBall {
 using vec3 = glm::vec3;
 using vec4 = glm::vec4;
+using mat4 = glm::mat4;
+inline const float* mat4_data(const mat4& m) { return &m[0][0]; }
 }  // namespace YarnBall
 #else
 namespace YarnBall {
@@ -42,6 +45,14 @@ struct vec4 {
     float& operator[](int i) { return (&x)[i]; }
     float operator[](int i) const { return (&x)[i]; }
 };
+// Column-major 4x4 matrix like glm::mat4: m[column][row]; mat4(d) is d times the identity.
+struct mat4 {
+    vec4 c[4];
+    explicit mat4(float d = 1.f) : c{vec4(d, 0, 0, 0), vec4(0, d, 0, 0), vec4(0, 0, d, 0), vec4(0, 0, 0, d)} {}
+    vec4& operator[](int i) { return c[i]; }
+    const vec4& operator[](int i) const { return c[i]; }
+};
+inline const float* mat4_data(const mat4& m) { return &m.c[0].x; }
 }  // namespace YarnBall
 #endif
 
@@ -129,14 +140,7 @@ class Sim {
 
     explicit Sim(int numVerts) {
         check(yb_create(numVerts, &h_));
-        yb_vertex* v = nullptr;
-        float *q = nullptr, *qr = nullptr, *vel = nullptr;
-        check(yb_host_arrays(h_, &v, &q, &qr, &vel));
-        verts = reinterpret_cast<Vertex*>(v);
-        qs = reinterpret_cast<Rotor*>(q);
-        qRests = reinterpret_cast<vec4*>(qr);
-        vels = reinterpret_cast<vec3*>(vel);
-        pull();
+        bind();
     }
     ~Sim() { yb_destroy(h_); }
     Sim(const Sim&) = delete;
@@ -213,10 +217,34 @@ class Sim {
         report_file(yb_export_obj(h_, path.c_str()));
     }
 
+    // Sim::glueEndpoints (io/jsonBuilder.cpp:174-212), on the host arrays.
+    void glueEndpoints(float searchRadius) {
+        push();
+        check(yb_glue_endpoints(h_, searchRadius));
+    }
+
     yb_sim* handle() { return h_; }
+
+    // A Sim around a handle made by the C ABI (the readers below).
+    static Sim* adopt(yb_sim* h) { return new Sim(h); }
 
    private:
     yb_sim* h_ = nullptr;
+
+    explicit Sim(yb_sim* h) : h_(h) { bind(); }
+    void bind() {
+        yb_vertex* v = nullptr;
+        float *q = nullptr, *qr = nullptr, *vel = nullptr;
+        check(yb_host_arrays(h_, &v, &q, &qr, &vel));
+        verts = reinterpret_cast<Vertex*>(v);
+        qs = reinterpret_cast<Rotor*>(q);
+        qRests = reinterpret_cast<vec4*>(qr);
+        vels = reinterpret_cast<vec3*>(vel);
+        pull();
+        const float* im = nullptr;
+        int32_t cnt = 0;
+        if (yb_initial_inv_masses(h_, &im, &cnt) == YB_OK && im) initialInvMasses.assign(im, im + cnt);
+    }
 
     static void check(yb_status st) {
         if (st != YB_OK) throw std::runtime_error(yb_status_string(st));
@@ -237,5 +265,44 @@ class Sim {
         check(yb_get_max_h(h_, &maxH));
     }
 };
+
+// ---- scene construction (io/reader.cpp:49-293, io/jsonBuilder.cpp:8-172) -----------------
+// Errors throw std::runtime_error with the reference's messages.
+namespace detail {
+inline Sim* adopt_or_throw(yb_status st, yb_sim* h) {
+    if (st != YB_OK) {
+        const char* m = yb_last_io_error();
+        throw std::runtime_error(m && *m ? m : yb_status_string(st));
+    }
+    return Sim::adopt(h);
+}
+}  // namespace detail
+
+inline Sim* readFromOBJ(std::string path, float targetSegLen, mat4 transform, bool breakUpClosedCurves = false,
+                        bool allowResample = true) {
+    yb_sim* h = nullptr;
+    const yb_status st = yb_read_obj(path.c_str(), targetSegLen, mat4_data(transform), breakUpClosedCurves,
+                                     allowResample, &h);
+    return detail::adopt_or_throw(st, h);
+}
+inline Sim* readFromBCC(std::string path, float targetSegLen, mat4 transform, bool breakUpClosedCurves = false,
+                        bool allowResample = true) {
+    yb_sim* h = nullptr;
+    const yb_status st = yb_read_bcc(path.c_str(), targetSegLen, mat4_data(transform), breakUpClosedCurves,
+                                     allowResample, &h);
+    return detail::adopt_or_throw(st, h);
+}
+inline Sim* readFromPoly(std::string path, float targetSegLen, mat4 transform, bool breakUpClosedCurves = false,
+                         bool allowResample = true) {
+    yb_sim* h = nullptr;
+    const yb_status st = yb_read_poly(path.c_str(), targetSegLen, mat4_data(transform), breakUpClosedCurves,
+                                      allowResample, &h);
+    return detail::adopt_or_throw(st, h);
+}
+inline Sim* buildFromJSON(std::string path) {
+    yb_sim* h = nullptr;
+    const yb_status st = yb_build_from_json(path.c_str(), &h);
+    return detail::adopt_or_throw(st, h);
+}
 
 }  // namespace YarnBall

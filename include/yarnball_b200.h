@@ -43,7 +43,9 @@ typedef enum yb_status {
     YB_ERR_OUT_OF_MEMORY = 10,
     YB_ERR_INTERNAL = 11,              /* a bounded device wait expired or the BVH stack overflowed */
     YB_ERR_ALREADY_CONFIGURED = 12,
-    YB_ERR_SCRATCH_TOO_SMALL = 13      /* request larger than a fixed scratch area */
+    YB_ERR_SCRATCH_TOO_SMALL = 13,     /* request larger than a fixed scratch area */
+    YB_ERR_IO = 14,                    /* a file could not be opened (io/reader.cpp, io/jsonBuilder.cpp) */
+    YB_ERR_FORMAT = 15                 /* a file could not be parsed; yb_last_io_error() has the message */
 } yb_status;
 
 /* VertexFlags, YarnBall.h:34-40 */
@@ -254,6 +256,47 @@ yb_status yb_export_obj(yb_sim* sim, const char* path);
  * Pin motions (yb_set_pin_motion) are not saved.  Requires a configured simulation. */
 yb_status yb_save_state(yb_sim* sim, const char* path);
 yb_status yb_load_state(const char* path, yb_sim** out);
+
+/* ---- scene construction from files (io/reader.cpp, io/resample.h, io/jsonBuilder.cpp) ----
+ * readFromBCC / readFromOBJ / readFromPoly: curves from a file, each point mapped by
+ * `transform` (4x4, column major like glm::mat4; NULL = identity) as vec3(T * vec4(p, 1)),
+ * Catmull-Rom curves resampled to about `targetSegLen` spacing when allowResample is set, and
+ * turned into a new, unconfigured simulation by createFromCurves (io/reader.cpp:13-47): one
+ * yarn per curve, closed curves glued end to end through connectionIndex unless
+ * breakUpClosedCurves.  Curves that end up with fewer than 3 (.bcc) or 4 (.obj, .poly) points
+ * are dropped.  A file that cannot be opened gives YB_ERR_IO and a malformed one
+ * YB_ERR_FORMAT; yb_last_io_error() returns the reference's exception message for either. */
+yb_status yb_read_bcc(const char* path, float targetSegLen, const float transform[16], int32_t breakUpClosedCurves,
+                      int32_t allowResample, yb_sim** out);
+yb_status yb_read_obj(const char* path, float targetSegLen, const float transform[16], int32_t breakUpClosedCurves,
+                      int32_t allowResample, yb_sim** out);
+yb_status yb_read_poly(const char* path, float targetSegLen, const float transform[16], int32_t breakUpClosedCurves,
+                       int32_t allowResample, yb_sim** out);
+
+/* buildFromJSON (io/jsonBuilder.cpp:8-172): reads the scene description (curveFile,
+ * transform (3x4 rows; default scale 0.01), resampleLength, breakUpClosedCurves, curveRadius,
+ * the "simulation" block, glueEndpoints, fixBorders, fixVertex), then configures, sets
+ * kStretch/kBend, glues, pins and uploads.  The file may hold // and block comments and
+ * trailing commas.  Relative curve paths are relative to the working directory. */
+yb_status yb_build_from_json(const char* path, yb_sim** out);
+
+/* Sim::glueEndpoints (io/jsonBuilder.cpp:174-212) on the host arrays: every yarn endpoint is
+ * joined (connectionIndex both ways, both moved to their midpoint) to the nearest vertex of its
+ * scene with |i - j| > 2 when that vertex is within searchRadius and neither is joined yet.
+ * The nearest-vertex search runs on the GPU over the positions at the call (ties: the lowest
+ * index); joins are applied in ascending endpoint order. */
+yb_status yb_glue_endpoints(yb_sim* sim, float searchRadius);
+
+/* Resample::resampleCMR (io/resample.h:143-187): `count` float xyz points of a uniform
+ * Catmull-Rom curve resampled between parameters start and end to about targetSegLen spacing.
+ * *outCount receives the number of points; they are written to `out` when capacity allows
+ * (else YB_ERR_SCRATCH_TOO_SMALL; out = NULL only queries the count).  Curves with fewer than 4
+ * points are returned unchanged. */
+yb_status yb_resample_cmr(const float* points, int32_t count, double start, double end, double targetSegLen,
+                          float* out, int32_t capacity, int32_t* outCount);
+
+/* Message of the last failed file reader or JSON build on the calling thread. */
+const char* yb_last_io_error(void);
 
 /* First vertex and vertex count of a scene. */
 yb_status yb_scene_range(yb_sim* sim, int32_t scene, int32_t* first, int32_t* count);

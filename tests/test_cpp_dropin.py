@@ -39,3 +39,28 @@ def test_dropin_readme_matches_python(tmp_path):
     sim.download()
     assert np.array_equal(sim.verts["pos"][31], p31)
     assert np.array_equal(sim.verts["pos"][63], p63)
+
+
+def test_dropin_readers(tmp_path):
+    """YarnBall::readFromPoly through the drop-in header (no GPU needed) matches the Python
+    reader, and a malformed file throws with the reference's message."""
+    from tests.test_curves_cpu import _helix, _poly_text
+    from yarnball_b200 import sim as ybsim
+
+    exe = str(tmp_path / "reader_example")
+    cmd = ["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"),
+           os.path.join(ROOT, "tests", "cpp", "reader_example.cpp"),
+           "-L", os.path.join(ROOT, "yarnball_b200", "_lib"), "-lyarnball_b200",
+           "-Wl,-rpath," + os.path.join(ROOT, "yarnball_b200", "_lib"), "-o", exe]
+    subprocess.run(cmd, check=True, capture_output=True)
+    poly = tmp_path / "c.poly"
+    poly.write_text(_poly_text([_helix(40, seed=1) * 20], [_helix(25, turns=1, pitch=0.0, seed=2)[:-1] * 20]))
+    out = subprocess.run([exe, "poly", str(poly)], check=True, capture_output=True, text=True).stdout.split()
+    sim = ybsim.readFromPoly(str(poly), 2e-3, np.diag([0.01, 0.01, 0.01, 1.0]))
+    assert int(out[0]) == sim.numVerts and int(out[1]) == 2
+    assert np.array_equal(np.float32([float(x) for x in out[2:5]]), sim.verts["pos"][0])
+    sim.close()
+    bad = tmp_path / "bad.poly"
+    bad.write_text("POINTS\n1: 0 0 0\n2: 1 0 0\n3: 0 1 0\n4: 0 0 1\nPOLYS\n1: 1 2\n2: 1 3\n3: 1 4\nEND\n")
+    r = subprocess.run([exe, "poly", str(bad)], capture_output=True, text=True)
+    assert r.returncode == 1 and r.stdout.strip() == "error: Graphs not allowed."

@@ -184,25 +184,33 @@ def test_batched_equals_alone():
 
 def test_device_pin_driver_follows_prescribed_rotation():
     """The device-side kinematic driver places driven pins exactly on the prescribed rotation
-    (the reference's twist scenario, KittenEngine/main.cpp:54-87) and agrees with the
-    host-side download/move/upload driver after one frame."""
+    (the reference's twist scenario, KittenEngine/main.cpp:54-87, rotateY about +y) and agrees
+    with the host-side download/move/upload driver after one frame.  The comparison stops
+    after one frame: from the second frame on the host driver's upload() clears every
+    vertex's Kahan compensation term (about 1e-7 m at y = 1 m) while the device driver clears
+    only the driven pins', and the twisted bundle buckles, which amplifies that difference."""
     a = scenes.build_twist(grid=3, verts=512)
     b = scenes.build_twist(grid=3, verts=512)
     x0 = a.read_state_f64()[0]
     groups, center = scenes.device_twist(a, omega=2 * np.pi)
     drv = scenes.TwistDriver(b, omega=2 * np.pi)
-    frames = 3
-    for _ in range(frames):
-        a.advance(1 / 30.0)
-        drv.frame(1 / 30.0)
+    a.advance(1 / 30.0)
+    drv.frame(1 / 30.0)
     pa = a.read_state_f64()[0]
     pb = b.read_state_f64()[0]
+    disp = np.abs(pb - x0).max()
+    assert disp > 0
+    assert np.abs(pa - pb).max() <= 1e-4 * disp
+    frames = 3
+    for _ in range(frames - 1):
+        a.advance(1 / 30.0)
+    pa = a.read_state_f64()[0]
     top = groups == 1
     # driven pins at the start of the last frame plus h v over its substeps = rotation at t = frames/30
     ang = 2 * np.pi * frames / 30.0
     c, s = np.cos(ang), np.sin(ang)
     d = x0[top] - center
-    expect = np.stack([c * d[:, 0] - s * d[:, 2], d[:, 1], s * d[:, 0] + c * d[:, 2]], 1) + center
+    expect = np.stack([c * d[:, 0] + s * d[:, 2], d[:, 1], -s * d[:, 0] + c * d[:, 2]], 1) + center
     assert np.abs(pa[top] - expect).max() < 2e-6
-    disp = np.abs(pb - x0).max()
-    assert np.abs(pa - pb).max() <= 1e-3 * disp
+    a.close()
+    b.close()

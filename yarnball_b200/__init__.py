@@ -4,4 +4,5 @@ The engine is the CUDA library yarnball_b200/_lib/libyarnball_b200.so (C ABI dec
 include/yarnball_b200.h).  This package is the Python mirror of YarnBall::Sim over that ABI.
 """
 from ._abi import YarnBallError, load  # noqa: F401
-from .sim import MAX_COLLISIONS_PER_SEGMENT, Sim, VertexFlags, sort_pairs  # noqa: F401
+from .sim import (MAX_COLLISIONS_PER_SEGMENT, Sim, VertexFlags, buildFromJSON, readFromBCC,  # noqa: F401
+                  readFromOBJ, readFromPoly, resampleCMR, sort_pairs)

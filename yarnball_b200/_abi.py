@@ -119,6 +119,17 @@ SIGNATURES = {
     "yb_export_bcc": (ctypes.c_int, [_P, ctypes.c_char_p, ctypes.c_int32]),
     "yb_export_obj": (ctypes.c_int, [_P, ctypes.c_char_p]),
     "yb_save_state": (ctypes.c_int, [_P, ctypes.c_char_p]),
+    "yb_read_bcc": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_float, c_float_p, ctypes.c_int32, ctypes.c_int32,
+                                   ctypes.POINTER(_P)]),
+    "yb_read_obj": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_float, c_float_p, ctypes.c_int32, ctypes.c_int32,
+                                   ctypes.POINTER(_P)]),
+    "yb_read_poly": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_float, c_float_p, ctypes.c_int32, ctypes.c_int32,
+                                    ctypes.POINTER(_P)]),
+    "yb_build_from_json": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_P)]),
+    "yb_glue_endpoints": (ctypes.c_int, [_P, ctypes.c_float]),
+    "yb_resample_cmr": (ctypes.c_int, [c_float_p, ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                       c_float_p, ctypes.c_int32, c_int32_p]),
+    "yb_last_io_error": (ctypes.c_char_p, []),
     "yb_load_state": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_P)]),
     "yb_set_pin_motion": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint8), ctypes.c_int32,
                                          ctypes.POINTER(YbPinMotion)]),

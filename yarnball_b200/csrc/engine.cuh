@@ -94,7 +94,8 @@ template <typename R>
 struct alignas(16) BNode {         // internal BVH node: boxes of both children + links
     R lmin[3], lmax[3], rmin[3], rmax[3];
     int left, right;               // child code: >= 0 internal node, < 0 leaf -(seg + 1)
-    int parent, pad;
+    int parent;
+    int split;                     // sorted position of the left child's last leaf
 };
 
 template <typename R>
@@ -123,7 +124,9 @@ struct Dev {
     int* leafParent;  // per sorted leaf position
     unsigned* refitCount;
     int* sceneRoot;   // child code of each scene's subtree root (or INT_MIN when empty)
-    int* sceneSegOff; // numScenes + 1 prefix of segments per scene
+    int* sceneLast;   // sorted position of the last leaf of each scene's subtree
+    unsigned* travNext;   // next query (sorted position) handed out by the traversal
+    int travBlocks;       // persistent traversal grid
     unsigned long long* keys[2];
     int* vals[2];
     unsigned* sceneBox;   // 6 ordered-uint per scene: min xyz, max xyz of segment midpoints
@@ -136,6 +139,7 @@ template <typename R> void launch_iter(const Dev<R>& d, int srcBuf, int threads,
 template <typename R> void launch_bvh_rebuild(const Dev<R>& d, cudaStream_t s, void* sortScratch, size_t sortScratchBytes, int keyBits);
 template <typename R> void launch_bvh_refit(const Dev<R>& d, cudaStream_t s);
 template <typename R> void launch_traverse(const Dev<R>& d, cudaStream_t s);  // + list sort + step limit (2 kernels)
+template <typename R> int traverse_blocks_per_sm();  // resident traversal blocks per SM (persistent grid)
 template <typename R> void launch_lists_step_limit(const Dev<R>& d, cudaStream_t s);  // step limit over segments
 template <typename R> void launch_bvh_reset(const Dev<R>& d, cudaStream_t s);
 // Places driven vertices on their prescribed motion at the start of an advance of length dt.

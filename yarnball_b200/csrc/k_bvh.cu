@@ -134,6 +134,7 @@ __global__ void __launch_bounds__(256) k_karras(Dev<R> d, const unsigned long lo
     const int gamma = i + s * dir + (dir < 0 ? -1 : 0);
     const int first = min(i, j), last = max(i, j);
     BNode<R>& nd = d.nodes[i];
+    nd.split = gamma;
     if (first == gamma) {
         nd.left = -(vals[gamma] + 1);
         d.leafParent[gamma] = i;
@@ -151,8 +152,10 @@ __global__ void __launch_bounds__(256) k_karras(Dev<R> d, const unsigned long lo
     if (i == 0) nd.parent = -1;
     const unsigned long long sc = keys[first] >> 30;
     if ((keys[last] >> 30) == sc && (first == 0 || (keys[first - 1] >> 30) != sc) &&
-        (last == n - 1 || (keys[last + 1] >> 30) != sc))
+        (last == n - 1 || (keys[last + 1] >> 30) != sc)) {
         d.sceneRoot[sc] = i;
+        d.sceneLast[sc] = last;
+    }
 }
 
 template <typename R>
@@ -211,7 +214,6 @@ constexpr int BVH_STACK = 64;
 constexpr int TRAV_THREADS = 128;
 constexpr int TRAV_WARPS = TRAV_THREADS / 32;
 constexpr int TRAV_QCAP = 96;       // < 32 left over + up to 2 candidates per lane
-constexpr int TRAV_JBITS = 26;      // candidate entry = (owner lane << 26) | partner segment
 
 // Appends y to x's contact list.  The count keeps growing past MAX_COLS so that the list
 // kernel can report the overflow (collision.cu:80-90).
@@ -221,122 +223,131 @@ __device__ __forceinline__ void list_append(const Dev<R>& d, int x, int y) {
     if (pos < MAX_COLS) d.cols[x + (size_t)d.n * pos] = y;
 }
 
-// Broadphase + narrow phase, one warp per 32 query segments taken in Morton order (the sorted
-// leaves of the last rebuild), so a warp's queries are spatially close.  The warp walks the
-// tree as a packet: every step loads one node (the same address in all lanes), each lane tests
-// the node's two child boxes against its own query box, and the warp descends into a child if
-// any lane overlaps it (warp-uniform control flow, one shared stack).  A leaf that overlaps a
-// lane's box and has a larger segment index than the lane's becomes a candidate pair in a
+// Broadphase + narrow phase.  Every segment queries the tree once with its own box (the
+// sorted leaves of the last rebuild, taken in Morton order, so neighbouring lanes start on
+// neighbouring queries).  Each unordered pair is found by exactly one of its two segments:
+// the one with the lower sorted position, whose walk skips every subtree holding only leaves
+// at or before its own position (node.split and the node's last position bound the children's
+// ranges; the last position travels on the lane's stack).  Lanes walk independently, with a
+// per-lane stack; a lane that finishes takes the next unprocessed query from a global counter
+// (one atomic per warp and refill), so a warp keeps all 32 lanes busy until the queries run
+// out (persistent grid).  A leaf that overlaps a lane's box becomes a candidate pair in a
 // per-warp queue; whenever 32 candidates are queued the warp runs the separately rounded
-// narrow-phase test on them, one pair per lane, and appends kept pairs to both lists.
-// A warp walks the subtree of its lanes' scene; the few warps that straddle a scene boundary
-// walk once per scene, each time with the other scene's lanes idle.
+// narrow-phase test on them, one pair per lane, with the lower segment index as segment A,
+// and appends kept pairs to both lists.  The pair set is the same as an all-pairs test: the
+// test is symmetric and every overlapping pair is visited once.
+template <typename R>
+__device__ __forceinline__ void trav_load_node(const BNode<R>* nodes, int node, BNode<R>& nd) {
+    if constexpr (sizeof(R) == 4) {  // one node = four 16-byte loads
+        const float4* src = reinterpret_cast<const float4*>(nodes + node);
+        float4* dst = reinterpret_cast<float4*>(&nd);
+        dst[0] = __ldg(src); dst[1] = __ldg(src + 1); dst[2] = __ldg(src + 2); dst[3] = __ldg(src + 3);
+    } else {
+        nd = nodes[node];
+    }
+}
+
 template <typename R>
 __global__ void __launch_bounds__(TRAV_THREADS) k_traverse(Dev<R> d) {
-    __shared__ int sQ[TRAV_WARPS][TRAV_QCAP];
-    __shared__ int sSeg[TRAV_WARPS][32];
-    __shared__ int sScene[TRAV_WARPS][32];
-    __shared__ int sStack[TRAV_WARPS][BVH_STACK];
+    __shared__ int sQx[TRAV_WARPS][TRAV_QCAP];
+    __shared__ int sQy[TRAV_WARPS][TRAV_QCAP];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int si = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool active = si < d.nseg;
-    int k = -1, sc = -1;
-    Box<R> qb;
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-        qb.mn[a] = yinf<R>();
-        qb.mx[a] = -yinf<R>();
-    }
-    if (active) {
-        k = d.vals[0][si];
-        sc = scene_of(d.vp[k].flags);
-        qb = segment_box(d, k, d.sp[sc]);
-    }
-    sSeg[warp][lane] = k;
-    sScene[warp][lane] = sc;
-    unsigned todo = __ballot_sync(0xffffffffu, active);
-    if (todo == 0u || d.nseg < 2) return;  // (warp-uniform)
     const unsigned lt = (1u << lane) - 1u;
-    int qn = 0;  // queued candidates (identical in every lane)
-    __syncwarp();
-    // One packet walk per distinct scene among the lanes (almost always one): lanes of other
-    // scenes take part with an empty query box.
-    while (todo) {
-    const int scw = __shfl_sync(0xffffffffu, sc, __ffs(todo) - 1);
-    const bool mine = active && sc == scw;
-    todo &= ~__ballot_sync(0xffffffffu, mine);
-    Box<R> pb = qb;
-    if (!mine) {
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-            pb.mn[a] = yinf<R>();
-            pb.mx[a] = -yinf<R>();
-        }
-    }
-    int node = d.sceneRoot[scw];
-    bool done = node < 0;  // a scene of one segment has no pairs
+    const int nseg = d.nseg;
+    int2 stack[BVH_STACK];
     int top = 0;
+    int qi = 0, k = -1, node = -1, last = -1;  // query: sorted position, segment, walk state
+    int steps = 0;        // nodes visited by this query (a valid walk visits fewer than nseg)
+    bool walking = false;
+    Box<R> qb;
+    int qn = 0;           // queued candidates (identical in every lane)
+    bool more = true;     // the counter has not run out (warp-uniform)
     while (true) {
-        int c0 = -1, c1 = -1;
-        if (!done) {
-            BNode<R> nd;
-            if constexpr (sizeof(R) == 4) {  // one node = four 16-byte loads, same address in every lane
-                const float4* src = reinterpret_cast<const float4*>(d.nodes + node);
-                float4* dst = reinterpret_cast<float4*>(&nd);
-                dst[0] = __ldg(src); dst[1] = __ldg(src + 1); dst[2] = __ldg(src + 2); dst[3] = __ldg(src + 3);
-            } else {
-                nd = d.nodes[node];
+        // Refill lanes without a walk.
+        const unsigned idle = __ballot_sync(0xffffffffu, !walking);
+        if (more && idle) {
+            int base = 0;
+            if (lane == 0) base = (int)atomicAdd(d.travNext, (unsigned)__popc(idle));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base + __popc(idle) >= nseg) more = false;
+            if (!walking) {
+                qi = base + __popc(idle & lt);
+                if (qi < nseg) {
+                    k = d.vals[0][qi];
+                    const int sc = scene_of(d.vp[k].flags);
+                    qb = segment_box(d, k, d.sp[sc]);
+                    node = d.sceneRoot[sc];
+                    last = d.sceneLast[sc];
+                    top = 0;
+                    steps = 0;
+                    walking = node >= 0 && last > qi;  // a leaf root has no pairs
+                }
             }
-            const bool ol = box_overlap(pb, nd.lmin, nd.lmax);
-            const bool orr = box_overlap(pb, nd.rmin, nd.rmax);
+        }
+        if (!more && !__any_sync(0xffffffffu, walking) && qn == 0) break;
+        int c0 = -1, c1 = -1;
+        if (walking && (node >= nseg - 1 || ++steps > nseg)) {  // only a corrupt tree gets here
+            atomicOr(&d.err[EW_INTERNAL], IE_BVH_STACK);
+            walking = false;
+        }
+        if (walking) {
+            BNode<R> nd;
+            trav_load_node(d.nodes, node, nd);
+            const int g = nd.split;
+            bool ol = g > qi && box_overlap(qb, nd.lmin, nd.lmax);
+            bool orr = last > qi && box_overlap(qb, nd.rmin, nd.rmax);
             const int L = nd.left, Rc = nd.right;
-            if (ol && L < 0 && -L - 1 > k) c0 = -L - 1;
-            if (orr && Rc < 0 && -Rc - 1 > k) c1 = -Rc - 1;
-            const bool goL = __any_sync(0xffffffffu, ol && L >= 0);
-            const bool goR = __any_sync(0xffffffffu, orr && Rc >= 0);
-            if (goL && goR) {
+            if (ol && L < 0) { c0 = -L - 1; ol = false; }
+            if (orr && Rc < 0) { c1 = -Rc - 1; orr = false; }
+            if (ol && orr) {
                 if (top < BVH_STACK) {
-                    if (lane == 0) sStack[warp][top] = Rc;
-                    top++;
-                } else if (lane == 0) {
+                    stack[top++] = make_int2(Rc, last);
+                } else {
                     atomicOr(&d.err[EW_INTERNAL], IE_BVH_STACK);
                 }
                 node = L;
-            } else if (goL) {
+                last = g;
+            } else if (ol) {
                 node = L;
-            } else if (goR) {
+                last = g;
+            } else if (orr) {
                 node = Rc;
             } else if (top > 0) {
-                __syncwarp();
-                node = sStack[warp][--top];
+                const int2 e = stack[--top];
+                node = e.x;
+                last = e.y;
             } else {
-                done = true;
+                walking = false;
             }
-            __syncwarp();
         }
         const unsigned b0 = __ballot_sync(0xffffffffu, c0 >= 0);
         const unsigned b1 = __ballot_sync(0xffffffffu, c1 >= 0);
-        if (c0 >= 0) sQ[warp][qn + __popc(b0 & lt)] = (lane << TRAV_JBITS) | c0;
-        if (c1 >= 0) sQ[warp][qn + __popc(b0) + __popc(b1 & lt)] = (lane << TRAV_JBITS) | c1;
+        if (c0 >= 0) {
+            const int at = qn + __popc(b0 & lt);
+            sQx[warp][at] = min(k, c0);
+            sQy[warp][at] = max(k, c0);
+        }
+        if (c1 >= 0) {
+            const int at = qn + __popc(b0) + __popc(b1 & lt);
+            sQx[warp][at] = min(k, c1);
+            sQy[warp][at] = max(k, c1);
+        }
         qn += __popc(b0) + __popc(b1);
         __syncwarp();
-        while (qn >= 32 || (done && qn > 0)) {
+        const bool drain = !more && !__any_sync(0xffffffffu, walking);
+        while (qn >= 32 || (drain && qn > 0)) {
             const int m = min(qn, 32);
             if (lane < m) {
-                const int e = sQ[warp][qn - m + lane];
-                const int owner = e >> TRAV_JBITS;
-                const int j = e & ((1 << TRAV_JBITS) - 1);
-                const int x = sSeg[warp][owner];
-                if (pair_keep(d, x, j, d.sp[sScene[warp][owner]])) {
-                    list_append(d, x, j);
-                    list_append(d, j, x);
+                const int x = sQx[warp][qn - m + lane];
+                const int y = sQy[warp][qn - m + lane];
+                if (pair_keep(d, x, y, d.sp[scene_of(d.vp[x].flags)])) {
+                    list_append(d, x, y);
+                    list_append(d, y, x);
                 }
             }
             qn -= m;
             __syncwarp();
         }
-        if (done && qn == 0) break;
-    }
     }
 }
 
@@ -406,7 +417,9 @@ template <typename R>
 void launch_traverse(const Dev<R>& d, cudaStream_t s) {
     if (d.nseg <= 0) return;
     cudaMemsetAsync(d.numCols, 0, sizeof(int) * d.n, s);
-    k_traverse<R><<<(d.nseg + TRAV_THREADS - 1) / TRAV_THREADS, TRAV_THREADS, 0, s>>>(d);
+    cudaMemsetAsync(d.travNext, 0, sizeof(unsigned), s);
+    const int blocks = min((d.nseg + TRAV_THREADS - 1) / TRAV_THREADS, max(d.travBlocks, 1));
+    k_traverse<R><<<blocks, TRAV_THREADS, 0, s>>>(d);
     k_lists<R><<<(d.nseg + 127) / 128, 128, 0, s>>>(d, 1);
 }
 
@@ -422,6 +435,17 @@ template void launch_bvh_refit<float>(const Dev<float>&, cudaStream_t);
 template void launch_bvh_refit<double>(const Dev<double>&, cudaStream_t);
 template void launch_bvh_reset<float>(const Dev<float>&, cudaStream_t);
 template void launch_bvh_reset<double>(const Dev<double>&, cudaStream_t);
+template <typename R>
+int traverse_blocks_per_sm() {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_traverse<R>, TRAV_THREADS, 0) != cudaSuccess || b < 1) {
+        cudaGetLastError();
+        b = 4;
+    }
+    return b;
+}
+template int traverse_blocks_per_sm<float>();
+template int traverse_blocks_per_sm<double>();
 template void launch_traverse<float>(const Dev<float>&, cudaStream_t);
 template void launch_lists_step_limit<float>(const Dev<float>&, cudaStream_t);
 template void launch_lists_step_limit<double>(const Dev<double>&, cudaStream_t);

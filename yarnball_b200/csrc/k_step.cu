@@ -636,7 +636,7 @@ void launch_iter(const Dev<R>& d, int srcBuf, int threads, int lanes, int pipe, 
     if (lanes == 0) {  // load-balanced contact loop
         if constexpr (sizeof(R) == 4) {
             if (threads == 256)
-                k_iter_bal<R, 256, 3><<<(d.n + 253) / 254, 256, 0, s>>>(d, srcBuf);
+                k_iter_bal<R, 256, 4><<<(d.n + 253) / 254, 256, 0, s>>>(d, srcBuf);
             else
                 k_iter_bal<R, 128, 6><<<(d.n + 125) / 126, 128, 0, s>>>(d, srcBuf);
         } else {

@@ -345,6 +345,8 @@ struct Engine : EngineBase {
         want((void**)&d.leafParent, sizeof(int) * n);
         want((void**)&d.refitCount, sizeof(unsigned) * nn);
         want((void**)&d.sceneRoot, sizeof(int) * ns);
+        want((void**)&d.sceneLast, sizeof(int) * ns);
+        want((void**)&d.travNext, sizeof(unsigned) * 4);
         want((void**)&d.keys[0], sizeof(unsigned long long) * n);
         want((void**)&d.keys[1], sizeof(unsigned long long) * n);
         want((void**)&d.vals[0], sizeof(int) * n);
@@ -368,7 +370,12 @@ struct Engine : EngineBase {
         d.numScenes = S->numScenes;
         d.nseg = 0;
         d.sp = spDev;
-        d.sceneSegOff = nullptr;
+        {
+            int dev = 0, sms = 148;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            d.travBlocks = sms * traverse_blocks_per_sm<R>();
+        }
         YB_CUDA(cudaHostAlloc((void**)&spHost, sizeof(SceneParams<R>) * ns, cudaHostAllocDefault));
         YB_CUDA(cudaHostAlloc((void**)&errHost, sizeof(int) * EW_COUNT, cudaHostAllocDefault));
         YB_CUDA(cudaMemsetAsync(d.err, 0, sizeof(int) * EW_COUNT, S->stream));
@@ -1203,6 +1210,8 @@ const char* yb_status_string(yb_status s) {
         case YB_ERR_ALREADY_CONFIGURED: return "already configured";
         case YB_ERR_SCRATCH_TOO_SMALL:
             return "request exceeds the fixed scratch area of the allocation-free entry point (n > YB_SORT_NOALLOC_MAX_N)";
+        case YB_ERR_IO: return "Could not open file";
+        case YB_ERR_FORMAT: return "malformed file (see yb_last_io_error)";
     }
     return "unknown status";
 }

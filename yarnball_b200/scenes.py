@@ -162,11 +162,12 @@ class TwistDriver:
         self.t = 0.0
 
     def _rot(self, p, ang):
+        # rotateY of main.cpp:68-69 (right-handed about +y)
         c, s = math.cos(ang), math.sin(ang)
         d = p - self.center
         out = d.copy()
-        out[:, 0] = c * d[:, 0] - s * d[:, 2]
-        out[:, 2] = s * d[:, 0] + c * d[:, 2]
+        out[:, 0] = c * d[:, 0] + s * d[:, 2]
+        out[:, 2] = -s * d[:, 0] + c * d[:, 2]
         return out + self.center
 
     def frame(self, dt):

@@ -276,6 +276,11 @@ class Sim:
         check(lib.yb_load_state(os.fsencode(path), ctypes.byref(out)), "load_state")
         return Sim(_handle=out)
 
+    def glueEndpoints(self, searchRadius):
+        """Sim::glueEndpoints (io/jsonBuilder.cpp:174-212) on the host arrays; the nearest-vertex
+        search runs on the GPU, joins are applied in ascending endpoint order."""
+        check(self._lib.yb_glue_endpoints(self._h, float(searchRadius)), "glueEndpoints")
+
     def download_scene(self, scene):
         check(self._lib.yb_download_scene(self._h, int(scene)), "download_scene")
 
@@ -368,3 +373,69 @@ def sort_pairs(keys, vals, bits):
     check(lib.yb_debug_sort_pairs(ptr(k, ctypes.c_uint64), ptr(v, ctypes.c_int32), len(k), int(bits),
                                   ptr(ko, ctypes.c_uint64), ptr(vo, ctypes.c_int32)), "sort")
     return ko, vo
+
+
+# ---- scene construction from files (io/reader.cpp, io/jsonBuilder.cpp) --------------------
+
+def _io_check(status, where):
+    if status != 0:
+        msg = load_io_error()
+        raise _abi.YarnBallError(status, where + (": " + msg if msg else ""))
+
+
+def load_io_error():
+    m = _abi.load().yb_last_io_error()
+    return m.decode() if m else ""
+
+
+def _transform(transform):
+    """A 4x4 matrix in the usual row/column convention (applied as M @ [x, y, z, 1]) to the
+    column-major float layout of glm::mat4; None = identity."""
+    if transform is None:
+        return None
+    m = np.asarray(transform, np.float32).reshape(4, 4)
+    return np.ascontiguousarray(m.T.reshape(16))
+
+
+def _read(fn, path, targetSegLen, transform, breakUpClosedCurves, allowResample, where):
+    lib = _abi.load()
+    t = _transform(transform)
+    out = ctypes.c_void_p()
+    _io_check(getattr(lib, fn)(os.fsencode(path), float(targetSegLen), None if t is None else ptr(t, ctypes.c_float),
+                               int(bool(breakUpClosedCurves)), int(bool(allowResample)), ctypes.byref(out)), where)
+    return Sim(_handle=out)
+
+
+def readFromBCC(path, targetSegLen, transform=None, breakUpClosedCurves=False, allowResample=True):
+    """YarnBall::readFromBCC (io/reader.cpp:49-97): an unconfigured Sim with one yarn per curve."""
+    return _read("yb_read_bcc", path, targetSegLen, transform, breakUpClosedCurves, allowResample, "readFromBCC")
+
+
+def readFromOBJ(path, targetSegLen, transform=None, breakUpClosedCurves=False, allowResample=True):
+    """YarnBall::readFromOBJ (io/reader.cpp:99-156)."""
+    return _read("yb_read_obj", path, targetSegLen, transform, breakUpClosedCurves, allowResample, "readFromOBJ")
+
+
+def readFromPoly(path, targetSegLen, transform=None, breakUpClosedCurves=False, allowResample=True):
+    """YarnBall::readFromPoly (io/reader.cpp:158-293)."""
+    return _read("yb_read_poly", path, targetSegLen, transform, breakUpClosedCurves, allowResample, "readFromPoly")
+
+
+def buildFromJSON(path):
+    """YarnBall::buildFromJSON (io/jsonBuilder.cpp:8-172): a configured, uploaded Sim."""
+    out = ctypes.c_void_p()
+    _io_check(_abi.load().yb_build_from_json(os.fsencode(path), ctypes.byref(out)), "buildFromJSON")
+    return Sim(_handle=out)
+
+
+def resampleCMR(points, start, end, targetSegLen):
+    """Resample::resampleCMR (io/resample.h:143-187) on float xyz points."""
+    lib = _abi.load()
+    p = np.ascontiguousarray(np.asarray(points, np.float32).reshape(-1, 3))
+    cnt = ctypes.c_int32()
+    check(lib.yb_resample_cmr(ptr(p, ctypes.c_float), len(p), float(start), float(end), float(targetSegLen), None, 0,
+                              ctypes.byref(cnt)), "resampleCMR")
+    out = np.zeros((max(cnt.value, 1), 3), np.float32)
+    check(lib.yb_resample_cmr(ptr(p, ctypes.c_float), len(p), float(start), float(end), float(targetSegLen),
+                              ptr(out, ctypes.c_float), len(out), ctypes.byref(cnt)), "resampleCMR")
+    return out[:cnt.value]
