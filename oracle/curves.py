@@ -25,6 +25,8 @@ import struct
 
 import numpy as np
 
+HAS_NEXT = 2
+
 
 def _mix(x, y, a):
     return tuple(xi * (1.0 - a) + yi * a for xi, yi in zip(x, y))

@@ -172,3 +172,20 @@ def test_json_errors(tmp_path):
     missing = tmp_path / "m.json"
     missing.write_text('{ // a comment\n "curveFile": "/nonexistent-dir/c.poly", "resampleLength": 2e-3, }')
     assert lib.yb_build_from_json(str(missing).encode(), ctypes.byref(out)) == 14
+
+
+def test_glue_restatement_known_answer():
+    # yarn A: x axis 0..5 mm; yarn B starts 0.5 mm above A's vertex 3 and runs up the y axis.
+    a = np.stack([np.arange(6) * 1e-3, np.zeros(6), np.zeros(6)], 1)
+    b = np.stack([np.full(5, 3e-3), 5e-4 + np.arange(5) * 1e-3, np.zeros(5)], 1)
+    pos = np.concatenate([a, b]).astype(np.float32)
+    flags = np.full(11, 2, np.uint32)
+    flags[[5, 10]] = 0
+    cid = np.full(11, -1, np.int32)
+    p2, c2 = oc.glue_endpoints(pos, flags, cid, 1e-3)
+    # endpoints: 0 (A start), 5 (A end), 6 (B start), 10 (B end); only B's start is near A
+    assert c2[6] == 3 and c2[3] == 6 and (c2 >= 0).sum() == 2
+    np.testing.assert_array_equal(p2[6], np.float32([3e-3, 2.5e-4, 0]))
+    np.testing.assert_array_equal(p2[3], p2[6])
+    # a smaller radius joins nothing
+    assert (oc.glue_endpoints(pos, flags, cid, 4e-4)[1] >= 0).sum() == 0

@@ -98,6 +98,17 @@ struct alignas(16) BNode {         // internal BVH node: boxes of both children 
     int split;                     // sorted position of the left child's last leaf
 };
 
+// 4-wide view of the binary tree for traversal: entry e of node i is a grandchild of binary
+// node i (or a child, when that child is a leaf), with its box, child code and the sorted
+// position of the last leaf below it.  Unused entries have code WIDE_NONE and an empty box.
+constexpr int WIDE_NONE = -2147483647 - 1;
+template <typename R>
+struct alignas(16) WNode {
+    R mn[3][4], mx[3][4];
+    int code[4];
+    int last[4];
+};
+
 template <typename R>
 struct Dev {
     int n;            // vertices
@@ -121,6 +132,8 @@ struct Dev {
     int* err;         // EW_COUNT ints
     // BVH
     BNode<R>* nodes;  // nseg - 1 internal nodes
+    WNode<R>* wide;   // nseg - 1 wide nodes (rebuilt after every refit)
+    int* nodeLast;    // sorted position of the last leaf of each internal node's range
     int* leafParent;  // per sorted leaf position
     unsigned* refitCount;
     int* sceneRoot;   // child code of each scene's subtree root (or INT_MIN when empty)

@@ -135,6 +135,7 @@ __global__ void __launch_bounds__(256) k_karras(Dev<R> d, const unsigned long lo
     const int first = min(i, j), last = max(i, j);
     BNode<R>& nd = d.nodes[i];
     nd.split = gamma;
+    d.nodeLast[i] = last;
     if (first == gamma) {
         nd.left = -(vals[gamma] + 1);
         d.leafParent[gamma] = i;
@@ -210,10 +211,52 @@ __global__ void __launch_bounds__(256) k_refit(Dev<R> d, const int* __restrict__
     }
 }
 
-constexpr int BVH_STACK = 64;
+// Wide nodes from the refitted binary tree: node i's entries are the children of its two
+// children (a leaf child is an entry itself), so a walk over wide nodes loads one node per
+// two binary levels.  Entry order: left child's left, left child's right, right child's left,
+// right child's right.
+template <typename R>
+__global__ void __launch_bounds__(256) k_widen(Dev<R> d) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.nseg - 1) return;
+    const BNode<R> nd = d.nodes[i];
+    WNode<R> w;
+    int e = 0;
+    auto put = [&](int code, const R* mn, const R* mx, int last) {
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            w.mn[a][e] = mn[a];
+            w.mx[a][e] = mx[a];
+        }
+        w.code[e] = code;
+        w.last[e] = last;
+        e++;
+    };
+    const int lastI = d.nodeLast[i];
+    // left child covers [first, split], right child [split + 1, last]
+    const int kid[2] = {nd.left, nd.right};
+    const int kidLast[2] = {nd.split, lastI};
+    const R* kmn[2] = {nd.lmin, nd.rmin};
+    const R* kmx[2] = {nd.lmax, nd.rmax};
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+        if (kid[c] < 0) {
+            put(kid[c], kmn[c], kmx[c], kidLast[c]);
+            R emn[3] = {yinf<R>(), yinf<R>(), yinf<R>()}, emx[3] = {-yinf<R>(), -yinf<R>(), -yinf<R>()};
+            put(WIDE_NONE, emn, emx, -1);
+        } else {
+            const BNode<R>& ch = d.nodes[kid[c]];
+            put(ch.left, ch.lmin, ch.lmax, ch.split);
+            put(ch.right, ch.rmin, ch.rmax, kidLast[c]);
+        }
+    }
+    d.wide[i] = w;
+}
+
+constexpr int BVH_STACK = 96;
 constexpr int TRAV_THREADS = 128;
 constexpr int TRAV_WARPS = TRAV_THREADS / 32;
-constexpr int TRAV_QCAP = 96;       // < 32 left over + up to 2 candidates per lane
+constexpr int TRAV_QCAP = 160;      // < 32 left over + up to 4 candidates per lane
 
 // Appends y to x's contact list.  The count keeps growing past MAX_COLS so that the list
 // kernel can report the overflow (collision.cu:80-90).
@@ -226,24 +269,25 @@ __device__ __forceinline__ void list_append(const Dev<R>& d, int x, int y) {
 // Broadphase + narrow phase.  Every segment queries the tree once with its own box (the
 // sorted leaves of the last rebuild, taken in Morton order, so neighbouring lanes start on
 // neighbouring queries).  Each unordered pair is found by exactly one of its two segments:
-// the one with the lower sorted position, whose walk skips every subtree holding only leaves
-// at or before its own position (node.split and the node's last position bound the children's
-// ranges; the last position travels on the lane's stack).  Lanes walk independently, with a
-// per-lane stack; a lane that finishes takes the next unprocessed query from a global counter
-// (one atomic per warp and refill), so a warp keeps all 32 lanes busy until the queries run
-// out (persistent grid).  A leaf that overlaps a lane's box becomes a candidate pair in a
-// per-warp queue; whenever 32 candidates are queued the warp runs the separately rounded
-// narrow-phase test on them, one pair per lane, with the lower segment index as segment A,
-// and appends kept pairs to both lists.  The pair set is the same as an all-pairs test: the
-// test is symmetric and every overlapping pair is visited once.
+// the one with the lower sorted position, whose walk skips every entry holding only leaves at
+// or before its own position.  The walk runs over the wide nodes (four grandchildren per
+// node), so a query takes half as many dependent node loads as on the binary tree.  Lanes walk
+// independently, with a per-lane stack; a lane that finishes takes the next unprocessed query
+// from a global counter (one atomic per warp and refill), so a warp keeps all 32 lanes busy
+// until the queries run out (persistent grid).  A leaf entry that overlaps a lane's box
+// becomes a candidate pair in a per-warp queue; whenever 32 candidates are queued the warp
+// runs the separately rounded narrow-phase test on them, one pair per lane, with the lower
+// segment index as segment A, and appends kept pairs to both lists.  The pair set is the same
+// as an all-pairs test: the test is symmetric and every overlapping pair is visited once.
 template <typename R>
-__device__ __forceinline__ void trav_load_node(const BNode<R>* nodes, int node, BNode<R>& nd) {
-    if constexpr (sizeof(R) == 4) {  // one node = four 16-byte loads
-        const float4* src = reinterpret_cast<const float4*>(nodes + node);
-        float4* dst = reinterpret_cast<float4*>(&nd);
-        dst[0] = __ldg(src); dst[1] = __ldg(src + 1); dst[2] = __ldg(src + 2); dst[3] = __ldg(src + 3);
+__device__ __forceinline__ void trav_load_wide(const WNode<R>* wide, int node, WNode<R>& w) {
+    if constexpr (sizeof(R) == 4) {  // one wide node = eight 16-byte loads
+        const float4* src = reinterpret_cast<const float4*>(wide + node);
+        float4* dst = reinterpret_cast<float4*>(&w);
+#pragma unroll
+        for (int k = 0; k < 8; k++) dst[k] = __ldg(src + k);
     } else {
-        nd = nodes[node];
+        w = wide[node];
     }
 }
 
@@ -254,14 +298,14 @@ __global__ void __launch_bounds__(TRAV_THREADS) k_traverse(Dev<R> d) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     const int nseg = d.nseg;
-    int2 stack[BVH_STACK];
+    int stack[BVH_STACK];
     int top = 0;
-    int qi = 0, k = -1, node = -1, last = -1;  // query: sorted position, segment, walk state
-    int steps = 0;        // nodes visited by this query (a valid walk visits fewer than nseg)
+    int qi = 0, k = -1, node = -1;  // query: sorted position, segment, walk state
+    int steps = 0;                  // wide nodes visited by this query (a valid walk visits fewer than nseg)
     bool walking = false;
     Box<R> qb;
-    int qn = 0;           // queued candidates (identical in every lane)
-    bool more = true;     // the counter has not run out (warp-uniform)
+    int qn = 0;        // queued candidates (identical in every lane)
+    bool more = true;  // the counter has not run out (warp-uniform)
     while (true) {
         // Refill lanes without a walk.
         const unsigned idle = __ballot_sync(0xffffffffu, !walking);
@@ -277,62 +321,64 @@ __global__ void __launch_bounds__(TRAV_THREADS) k_traverse(Dev<R> d) {
                     const int sc = scene_of(d.vp[k].flags);
                     qb = segment_box(d, k, d.sp[sc]);
                     node = d.sceneRoot[sc];
-                    last = d.sceneLast[sc];
                     top = 0;
                     steps = 0;
-                    walking = node >= 0 && last > qi;  // a leaf root has no pairs
+                    walking = node >= 0 && d.sceneLast[sc] > qi;  // a leaf root has no pairs
                 }
             }
         }
         if (!more && !__any_sync(0xffffffffu, walking) && qn == 0) break;
-        int c0 = -1, c1 = -1;
+        int cand[4];
+        int nc = 0;
         if (walking && (node >= nseg - 1 || ++steps > nseg)) {  // only a corrupt tree gets here
             atomicOr(&d.err[EW_INTERNAL], IE_BVH_STACK);
             walking = false;
         }
         if (walking) {
-            BNode<R> nd;
-            trav_load_node(d.nodes, node, nd);
-            const int g = nd.split;
-            bool ol = g > qi && box_overlap(qb, nd.lmin, nd.lmax);
-            bool orr = last > qi && box_overlap(qb, nd.rmin, nd.rmax);
-            const int L = nd.left, Rc = nd.right;
-            if (ol && L < 0) { c0 = -L - 1; ol = false; }
-            if (orr && Rc < 0) { c1 = -Rc - 1; orr = false; }
-            if (ol && orr) {
-                if (top < BVH_STACK) {
-                    stack[top++] = make_int2(Rc, last);
+            WNode<R> w;
+            trav_load_wide(d.wide, node, w);
+            int next = -1;
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const bool hit = w.last[e] > qi && qb.mn[0] <= w.mx[0][e] && w.mn[0][e] <= qb.mx[0] &&
+                                 qb.mn[1] <= w.mx[1][e] && w.mn[1][e] <= qb.mx[1] && qb.mn[2] <= w.mx[2][e] &&
+                                 w.mn[2][e] <= qb.mx[2];
+                if (!hit) continue;
+                const int c = w.code[e];
+                if (c < 0) {
+                    cand[nc++] = -c - 1;
+                } else if (next < 0) {
+                    next = c;
+                } else if (top < BVH_STACK) {
+                    stack[top++] = c;
                 } else {
                     atomicOr(&d.err[EW_INTERNAL], IE_BVH_STACK);
                 }
-                node = L;
-                last = g;
-            } else if (ol) {
-                node = L;
-                last = g;
-            } else if (orr) {
-                node = Rc;
+            }
+            if (next >= 0) {
+                node = next;
             } else if (top > 0) {
-                const int2 e = stack[--top];
-                node = e.x;
-                last = e.y;
+                node = stack[--top];
             } else {
                 walking = false;
             }
         }
-        const unsigned b0 = __ballot_sync(0xffffffffu, c0 >= 0);
-        const unsigned b1 = __ballot_sync(0xffffffffu, c1 >= 0);
-        if (c0 >= 0) {
-            const int at = qn + __popc(b0 & lt);
-            sQx[warp][at] = min(k, c0);
-            sQy[warp][at] = max(k, c0);
+        // queue this lane's candidates at its offset (warp scan of the counts)
+        int incl = nc;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
         }
-        if (c1 >= 0) {
-            const int at = qn + __popc(b0) + __popc(b1 & lt);
-            sQx[warp][at] = min(k, c1);
-            sQy[warp][at] = max(k, c1);
+        const int at = qn + incl - nc;
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            if (e < nc) {
+                sQx[warp][at + e] = min(k, cand[e]);
+                sQy[warp][at + e] = max(k, cand[e]);
+            }
         }
-        qn += __popc(b0) + __popc(b1);
+        qn += __shfl_sync(0xffffffffu, incl, 31);
         __syncwarp();
         const bool drain = !more && !__any_sync(0xffffffffu, walking);
         while (qn >= 32 || (drain && qn > 0)) {
@@ -411,6 +457,7 @@ void launch_bvh_refit(const Dev<R>& d, cudaStream_t s) {
     if (d.nseg <= 1) return;
     cudaMemsetAsync(d.refitCount, 0, sizeof(unsigned) * (d.nseg - 1), s);
     k_refit<R><<<(d.nseg + 255) / 256, 256, 0, s>>>(d, d.vals[0]);
+    k_widen<R><<<(d.nseg - 1 + 255) / 256, 256, 0, s>>>(d);
 }
 
 template <typename R>

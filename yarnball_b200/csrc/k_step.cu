@@ -613,6 +613,220 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_bal(Dev<R> d, int src) {
     }
 }
 
+// Warp-balanced variant of k_iter_bal: each warp flattens the contact lists of its own 32
+// vertices (warp scan) and processes them 32 at a time, so the contact loop needs no block
+// barrier and warps of one block proceed independently; per vertex the contributions are still
+// summed in list order.
+template <typename R, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_iter_wbal(Dev<R> d, int src) {
+    constexpr int B = NT;
+    constexpr int CORE = B - 2;
+    constexpr int NW = NT / 32;
+    const int t = threadIdx.x;
+    const int k = blockIdx.x * CORE - 1 + t;
+    const int n = d.n;
+    const bool valid = (k >= 0) && (k < n);
+    const D2<R>* __restrict__ DX = d.dx[src];
+    const V4<R>* __restrict__ QO = d.q[src];
+
+    __shared__ R sFb[3][B];
+    __shared__ R sHb[6][B];
+    __shared__ R sSL[B];
+    __shared__ R sDX[3][B];
+    __shared__ R sSeg[12][B];  // p0, e = p1 - p0, dx, dx1 of each slot's segment
+    __shared__ R sCon[18][B];  // contributions of one chunk of contacts
+    __shared__ int sOffW[NW][33];
+    __shared__ int sScene[B];
+
+    V3<R> fa(R(0)), fb(R(0));
+    H3<R> Ha, Hb;
+    Ha.zero(); Hb.zero();
+    R sl = yinf<R>();
+    uint32_t flags = 0;
+    R invMass = R(0), lRest = R(1), kStretch = R(0);
+    V3<R> p0(R(0)), p1(R(0)), dx(R(0)), dx1(R(0));
+    Q<R> q0 = qmk(R(0), R(0), R(0), R(1));
+    const SceneParams<R>* spp = d.sp;
+    int nc = 0, sc = 0;
+
+    if (valid) {
+        const VP<R> vp = d.vp[k];
+        flags = vp.flags;
+        lRest = vp.lRest;
+        kStretch = vp.kStretch;
+        sc = scene_of(flags);
+        spp = &d.sp[sc];
+        const SceneParams<R>& sp = *spp;
+        const V4<R> P = d.pos[k];
+        p0 = xyz(P);
+        invMass = P.w;
+        const D2<R> own = DX[k];
+        dx = xyz(own.a);
+        dx1 = xyz(own.b);
+        q0 = qof(QO[k]);
+        const R D = sp.D;
+        if (invMass != R(0)) {
+            const V4<R> v = d.vel[k];
+            const R hh = sp.hh;
+            const V3<R> y(sp.h * v.x + hh * sp.gx, sp.h * v.y + hh * sp.gy, sp.h * v.z + hh * sp.gz);
+            Ha.diag(R(1) / (invMass * hh));
+            fa = (R(1) / (hh * invMass)) * (y - dx);
+        }
+        if (vp.cid >= 0) {
+            const R stiff = R(40);
+            const V3<R> pc = xyz(d.pos[vp.cid]);
+            const V3<R> dc = xyz(DX[vp.cid].a);
+            fa -= stiff * ((p0 - pc) + (dx - dc) + D * dx);
+            Ha.add_diag(stiff * (R(1) + D));
+        }
+        if (flags & F_HAS_NEXT) {
+            p1 = xyz(d.pos[k + 1]);
+            sl = d.stepLim[k];
+            nc = d.numCols[k];
+            const R invl = R(1) / lRest;
+            const V3<R> c = ((p1 - p0) + (dx1 - dx)) * invl - qrotate(q0, V3<R>(R(1), R(0), R(0)));
+            const R ks = kStretch * invl;
+            R dd = ks * invl;
+            fa += ks * c - (D * dd) * dx;
+            fb += -ks * c - (D * dd) * dx1;
+            dd *= R(1) + D;
+            Ha.add_diag(dd);
+            Hb.add_diag(dd);
+        }
+    }
+    const V3<R> e = p1 - p0;
+    sSeg[0][t] = p0.x; sSeg[1][t] = p0.y; sSeg[2][t] = p0.z;
+    sSeg[3][t] = e.x; sSeg[4][t] = e.y; sSeg[5][t] = e.z;
+    sSeg[6][t] = dx.x; sSeg[7][t] = dx.y; sSeg[8][t] = dx.z;
+    sSeg[9][t] = dx1.x; sSeg[10][t] = dx1.y; sSeg[11][t] = dx1.z;
+    sScene[t] = sc;
+    // warp exclusive scan of the contact counts: each warp flattens its own 32 vertices
+    const int lane = t & 31, wp = t >> 5, w0 = wp << 5;
+    int incl = nc;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    sOffW[wp][lane] = incl - nc;
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    if (lane == 31) sOffW[wp][32] = total;
+    __syncwarp();
+    const int myOff = incl - nc;
+    for (int base = 0; base < total; base += 32) {
+        const int f = base + lane;
+        V3<R> cfa(R(0)), cfb(R(0));
+        H3<R> cHa, cHb;
+        cHa.zero(); cHb.zero();
+        if (f < total) {
+            int lo = 0, hi = 31;  // owner: the last lane of the warp whose offset is <= f
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (sOffW[wp][mid] <= f) lo = mid; else hi = mid - 1;
+            }
+            const int s = w0 + lo, c = f - sOffW[wp][lo];
+            const int ks = blockIdx.x * CORE - 1 + s;
+            const size_t at = ks + (size_t)n * c;
+            const int j = __ldg(d.cols + at);
+            const V3<R> sp0(sSeg[0][s], sSeg[1][s], sSeg[2][s]);
+            V3<R> r0, r1;
+            if (c < RELCAP) {
+                const V4<R> A = d.relA[at];
+                const R2<R> Bq = d.relB[at];
+                r0 = V3<R>(A.x, A.y, A.z);
+                r1 = V3<R>(A.w, Bq.x, Bq.y);
+            } else {
+                r0 = xyz(d.pos[j]) - sp0;
+                r1 = xyz(d.pos[j + 1]) - sp0;
+            }
+            const D2<R> pd = DX[j];
+            const V3<R> se(sSeg[3][s], sSeg[4][s], sSeg[5][s]);
+            const V3<R> sdx(sSeg[6][s], sSeg[7][s], sSeg[8][s]);
+            const V3<R> sdx1(sSeg[9][s], sSeg[10][s], sSeg[11][s]);
+            contact_term(se, sdx, sdx1, r0, r1, xyz(pd.a), xyz(pd.b), d.sp[sScene[s]], cfa, cHa, cfb, cHb);
+        }
+        sCon[0][t] = cfa.x; sCon[1][t] = cfa.y; sCon[2][t] = cfa.z;
+        sCon[3][t] = cfb.x; sCon[4][t] = cfb.y; sCon[5][t] = cfb.z;
+#pragma unroll
+        for (int q = 0; q < 6; q++) {
+            sCon[6 + q][t] = cHa.d[q];
+            sCon[12 + q][t] = cHb.d[q];
+        }
+        __syncwarp();
+        const int f0 = max(myOff, base), f1 = min(myOff + nc, base + 32);
+        for (int g = f0; g < f1; g++) {
+            const int i = w0 + g - base;
+            fa += V3<R>(sCon[0][i], sCon[1][i], sCon[2][i]);
+            fb += V3<R>(sCon[3][i], sCon[4][i], sCon[5][i]);
+#pragma unroll
+            for (int q = 0; q < 6; q++) {
+                Ha.d[q] += sCon[6 + q][i];
+                Hb.d[q] += sCon[12 + q][i];
+            }
+        }
+        __syncwarp();
+    }
+
+    sFb[0][t] = fb.x; sFb[1][t] = fb.y; sFb[2][t] = fb.z;
+#pragma unroll
+    for (int q = 0; q < 6; q++) sHb[q][t] = Hb.d[q];
+    sSL[t] = sl;
+    __syncthreads();
+
+    V3<R> dxn = dx;
+    if (valid && t > 0) {
+        if (flags & F_HAS_PREV) {
+            fa += V3<R>(sFb[0][t - 1], sFb[1][t - 1], sFb[2][t - 1]);
+            H3<R> hp;
+#pragma unroll
+            for (int q = 0; q < 6; q++) hp.d[q] = sHb[q][t - 1];
+            Ha.add(hp);
+            sl = ymin(sl, sSL[t - 1]);
+        }
+        if (invMass != R(0)) {
+            dxn = dx + spp->accel * solve3(Ha, fa);
+            const R l = len(dxn);
+            if (l > sl && l > R(0)) dxn *= sl / l;
+        }
+    }
+    sDX[0][t] = dxn.x; sDX[1][t] = dxn.y; sDX[2][t] = dxn.z;
+    const bool core = valid && t >= 1 && t <= CORE;
+    __syncthreads();
+
+    if (core) {
+        const V3<R> dxb(sDX[0][t + 1], sDX[1][t + 1], sDX[2][t + 1]);
+        D2<R> o;
+        o.a = v4(dxn, R(0));
+        o.b = v4(k + 1 < n ? dxb : V3<R>(R(0)), R(0));
+        d.dx[src ^ 1][k] = o;
+        Q<R> qn = q0;
+        if (!(flags & F_FIX_ORI) && (flags & F_HAS_NEXT)) {
+            V3<R> v = ((p1 - p0) + (dxb - dxn)) * (R(1) / lRest);
+            v *= R(-2) * kStretch;
+            Q<R> b = qmk(R(0), R(0), R(0), R(0));
+            if (flags & F_HAS_PREV) {
+                const Q<R> qr = qof(d.qRest[k - 1]);
+                const Q<R> qq = qof(QO[k - 1]);
+                const R s = qdot(qmul(qinv(qq), q0), qr) > R(0) ? R(1) : R(-1);
+                b = qadd(b, qscale(s, qmul(qq, qr)));
+            }
+            if (flags & F_HAS_NEXT_ORI) {
+                const Q<R> qr = qof(d.qRest[k]);
+                const Q<R> qq = qof(QO[k + 1]);
+                const R s = qdot(qmul(qinv(q0), qq), qr) > R(0) ? R(1) : R(-1);
+                b = qadd(b, qscale(s, qmul(qq, qinv(qr))));
+            }
+            const R bl = qlen(b);
+            if (bl > R(0)) {
+                const R lambda = len(v) + bl;
+                const Q<R> vb1 = qmul(qmul(qmk(v, R(0)), b), qmk(R(1), R(0), R(0), R(0)));
+                qn = qnormalize(qadd(vb1, qscale(lambda, b)));
+            }
+        }
+        d.q[src ^ 1][k] = v4of(qn);
+    }
+}
+
 // ---------------------------------------------------------------------------------------
 template <typename R>
 void launch_init(const Dev<R>& d, cudaStream_t s) {
@@ -627,13 +841,23 @@ void launch_end(const Dev<R>& d, int finalBuf, bool copyQ, bool kahan, cudaStrea
 }
 
 // Newton iteration launch shapes: NT threads per block, T lanes per vertex, pipelined or not;
-// lanes = 0 selects the load-balanced kernel (one lane per vertex, flattened contact lists).
+// lanes = 0 selects a load-balanced kernel (one lane per vertex, flattened contact lists):
+// per block (pipe = 0) or per warp (pipe = 1).
 template <typename R>
 void launch_iter(const Dev<R>& d, int srcBuf, int threads, int lanes, int pipe, cudaStream_t s) {
     if (d.n <= 0) return;
 #define YB_ITER(NT, T, MINB, P) \
     k_iter<R, NT, T, MINB, P><<<(d.n + (NT / T) - 3) / ((NT / T) - 2), NT, 0, s>>>(d, srcBuf)
-    if (lanes == 0) {  // load-balanced contact loop
+    if (lanes == 0 && pipe) {  // warp-balanced contact loop
+        if constexpr (sizeof(R) == 4) {
+            if (threads == 256)
+                k_iter_wbal<R, 256, 4><<<(d.n + 253) / 254, 256, 0, s>>>(d, srcBuf);
+            else
+                k_iter_wbal<R, 128, 6><<<(d.n + 125) / 126, 128, 0, s>>>(d, srcBuf);
+        } else {
+            k_iter_wbal<R, 128, 2><<<(d.n + 125) / 126, 128, 0, s>>>(d, srcBuf);
+        }
+    } else if (lanes == 0) {  // block-balanced contact loop
         if constexpr (sizeof(R) == 4) {
             if (threads == 256)
                 k_iter_bal<R, 256, 4><<<(d.n + 253) / 254, 256, 0, s>>>(d, srcBuf);
