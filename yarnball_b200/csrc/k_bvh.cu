@@ -170,35 +170,8 @@ __device__ __forceinline__ void store_child_box(BNode<R>& nd, bool left, const B
     }
 }
 
-// Entry e of a wide node: a child code, its box and the sorted position of its last leaf.
-template <typename R>
-__device__ __forceinline__ void put_wide(WNode<R>& w, int e, int code, const Box<R>& b, int last) {
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-        w.mn[a][e] = b.mn[a];
-        w.mx[a][e] = b.mx[a];
-    }
-    w.code[e] = code;
-    w.last[e] = last;
-}
-
-template <typename R>
-__device__ __forceinline__ void put_wide_empty(WNode<R>& w, int e) {
-    Box<R> b;
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-        b.mn[a] = yinf<R>();
-        b.mx[a] = -yinf<R>();
-    }
-    put_wide(w, e, WIDE_NONE, b, -1);
-}
-
 // Bottom-up refit: leaf boxes from the current positions/velocity radius, unions upward.
-// refitCount must be zero on entry (cleared by the launcher).  The same pass fills the wide
-// nodes the traversal walks: node i's entries are its children's children (a leaf child is an
-// entry itself), in the order left-left, left-right, right-left, right-right.  A leaf writes
-// its own entry into its parent's wide node; the thread that completes a node (second arrival)
-// writes that node's two child boxes into its parent's wide node.
+// refitCount must be zero on entry (cleared by the launcher).
 template <typename R>
 __global__ void __launch_bounds__(256) k_refit(Dev<R> d, const int* __restrict__ sortedVals) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -210,7 +183,6 @@ __global__ void __launch_bounds__(256) k_refit(Dev<R> d, const int* __restrict__
     if (d.nseg == 1) return;
     int node = d.leafParent[p];
     int guard = 0;
-    bool leaf = true;
     while (node >= 0) {
         if (node >= d.nseg - 1) {  // only a corrupt tree gets here: report, touch nothing
             atomicOr(&d.err[EW_INTERNAL], IE_REFIT);
@@ -219,43 +191,66 @@ __global__ void __launch_bounds__(256) k_refit(Dev<R> d, const int* __restrict__
         BNode<R>& nd = d.nodes[node];
         const bool isLeft = (nd.left == code);
         store_child_box(nd, isLeft, b);
-        if (leaf) {
-            WNode<R>& w = d.wide[node];
-            put_wide(w, isLeft ? 0 : 2, code, b, p);
-            put_wide_empty(w, isLeft ? 1 : 3);
-            leaf = false;
-        }
         __threadfence();
         const unsigned old = atomicAdd(&d.refitCount[node], 1u);
         if (old == 0u) return;  // first arrival: the sibling finishes this node
         __threadfence();
         const R* omn = isLeft ? nd.rmin : nd.lmin;
         const R* omx = isLeft ? nd.rmax : nd.lmax;
-        Box<R> other;
 #pragma unroll
         for (int a = 0; a < 3; a++) {
-            other.mn[a] = __ldcg(omn + a);
-            other.mx[a] = __ldcg(omx + a);
-        }
-        const int pp = nd.parent;
-        if (pp >= 0 && pp < d.nseg - 1) {
-            const int e = (d.nodes[pp].left == node) ? 0 : 2;
-            WNode<R>& w = d.wide[pp];
-            put_wide(w, e, nd.left, isLeft ? b : other, nd.split);
-            put_wide(w, e + 1, nd.right, isLeft ? other : b, d.nodeLast[node]);
-        }
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-            b.mn[a] = ymin(b.mn[a], other.mn[a]);
-            b.mx[a] = ymax(b.mx[a], other.mx[a]);
+            b.mn[a] = ymin(b.mn[a], __ldcg(omn + a));
+            b.mx[a] = ymax(b.mx[a], __ldcg(omx + a));
         }
         code = node;
-        node = pp;
+        node = nd.parent;
         if (++guard > 4096) {  // a cycle would mean a corrupt tree: stop and report
             atomicOr(&d.err[EW_INTERNAL], IE_REFIT);
             return;
         }
     }
+}
+
+// Wide nodes from the refitted binary tree: node i's entries are the children of its two
+// children (a leaf child is an entry itself), so a walk over wide nodes loads one node per
+// two binary levels.  Entry order: left child's left, left child's right, right child's left,
+// right child's right.
+template <typename R>
+__global__ void __launch_bounds__(256) k_widen(Dev<R> d) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.nseg - 1) return;
+    const BNode<R> nd = d.nodes[i];
+    WNode<R> w;
+    int e = 0;
+    auto put = [&](int code, const R* mn, const R* mx, int last) {
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            w.mn[a][e] = mn[a];
+            w.mx[a][e] = mx[a];
+        }
+        w.code[e] = code;
+        w.last[e] = last;
+        e++;
+    };
+    const int lastI = d.nodeLast[i];
+    // left child covers [first, split], right child [split + 1, last]
+    const int kid[2] = {nd.left, nd.right};
+    const int kidLast[2] = {nd.split, lastI};
+    const R* kmn[2] = {nd.lmin, nd.rmin};
+    const R* kmx[2] = {nd.lmax, nd.rmax};
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+        if (kid[c] < 0) {
+            put(kid[c], kmn[c], kmx[c], kidLast[c]);
+            R emn[3] = {yinf<R>(), yinf<R>(), yinf<R>()}, emx[3] = {-yinf<R>(), -yinf<R>(), -yinf<R>()};
+            put(WIDE_NONE, emn, emx, -1);
+        } else {
+            const BNode<R>& ch = d.nodes[kid[c]];
+            put(ch.left, ch.lmin, ch.lmax, ch.split);
+            put(ch.right, ch.rmin, ch.rmax, kidLast[c]);
+        }
+    }
+    d.wide[i] = w;
 }
 
 constexpr int BVH_STACK = 96;
@@ -462,6 +457,7 @@ void launch_bvh_refit(const Dev<R>& d, cudaStream_t s) {
     if (d.nseg <= 1) return;
     cudaMemsetAsync(d.refitCount, 0, sizeof(unsigned) * (d.nseg - 1), s);
     k_refit<R><<<(d.nseg + 255) / 256, 256, 0, s>>>(d, d.vals[0]);
+    k_widen<R><<<(d.nseg - 1 + 255) / 256, 256, 0, s>>>(d);
 }
 
 template <typename R>

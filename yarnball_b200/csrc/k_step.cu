@@ -629,16 +629,14 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_wbal(Dev<R> d, int src) {
     const D2<R>* __restrict__ DX = d.dx[src];
     const V4<R>* __restrict__ QO = d.q[src];
 
+    __shared__ R sFb[3][B];
+    __shared__ R sHb[6][B];
+    __shared__ R sSL[B];
+    __shared__ R sDX[3][B];
     __shared__ R sSeg[12][B];  // p0, e = p1 - p0, dx, dx1 of each slot's segment
-    __shared__ R sAcc[18][B];  // per-vertex accumulators fa, fb, Ha, Hb during the contact loop
-    __shared__ R sBuf[18][B];  // contributions of one chunk of contacts, then the halo exchange
+    __shared__ R sCon[18][B];  // contributions of one chunk of contacts
     __shared__ int sOffW[NW][33];
     __shared__ int sScene[B];
-    R (*sCon)[B] = sBuf;
-    R (*sFb)[B] = sBuf;        // rows 0-2 (each warp only touches its own columns before the barrier)
-    R (*sHb)[B] = sBuf + 3;    // rows 3-8
-    R* sSL = sBuf[9];
-    R (*sDX)[B] = sBuf + 10;   // rows 10-12
 
     V3<R> fa(R(0)), fb(R(0));
     H3<R> Ha, Hb;
@@ -702,13 +700,6 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_wbal(Dev<R> d, int src) {
     sSeg[6][t] = dx.x; sSeg[7][t] = dx.y; sSeg[8][t] = dx.z;
     sSeg[9][t] = dx1.x; sSeg[10][t] = dx1.y; sSeg[11][t] = dx1.z;
     sScene[t] = sc;
-    sAcc[0][t] = fa.x; sAcc[1][t] = fa.y; sAcc[2][t] = fa.z;
-    sAcc[3][t] = fb.x; sAcc[4][t] = fb.y; sAcc[5][t] = fb.z;
-#pragma unroll
-    for (int q = 0; q < 6; q++) {
-        sAcc[6 + q][t] = Ha.d[q];
-        sAcc[12 + q][t] = Hb.d[q];
-    }
     // warp exclusive scan of the contact counts: each warp flattens its own 32 vertices
     const int lane = t & 31, wp = t >> 5, w0 = wp << 5;
     int incl = nc;
@@ -763,22 +754,17 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_wbal(Dev<R> d, int src) {
         }
         __syncwarp();
         const int f0 = max(myOff, base), f1 = min(myOff + nc, base + 32);
-        if (f0 < f1) {
+        for (int g = f0; g < f1; g++) {
+            const int i = w0 + g - base;
+            fa += V3<R>(sCon[0][i], sCon[1][i], sCon[2][i]);
+            fb += V3<R>(sCon[3][i], sCon[4][i], sCon[5][i]);
 #pragma unroll
-            for (int q = 0; q < 18; q++) {
-                R acc = sAcc[q][t];
-                for (int g = f0; g < f1; g++) acc += sCon[q][w0 + g - base];
-                sAcc[q][t] = acc;
+            for (int q = 0; q < 6; q++) {
+                Ha.d[q] += sCon[6 + q][i];
+                Hb.d[q] += sCon[12 + q][i];
             }
         }
         __syncwarp();
-    }
-    fa = V3<R>(sAcc[0][t], sAcc[1][t], sAcc[2][t]);
-    fb = V3<R>(sAcc[3][t], sAcc[4][t], sAcc[5][t]);
-#pragma unroll
-    for (int q = 0; q < 6; q++) {
-        Ha.d[q] = sAcc[6 + q][t];
-        Hb.d[q] = sAcc[12 + q][t];
     }
 
     sFb[0][t] = fb.x; sFb[1][t] = fb.y; sFb[2][t] = fb.z;
@@ -862,11 +848,15 @@ void launch_iter(const Dev<R>& d, int srcBuf, int threads, int lanes, int pipe, 
     if (d.n <= 0) return;
 #define YB_ITER(NT, T, MINB, P) \
     k_iter<R, NT, T, MINB, P><<<(d.n + (NT / T) - 3) / ((NT / T) - 2), NT, 0, s>>>(d, srcBuf)
-    if (lanes == 0 && pipe) {  // warp-balanced contact loop (shared memory bounds the block size)
-        if constexpr (sizeof(R) == 4)
-            k_iter_wbal<R, 128, 8><<<(d.n + 125) / 126, 128, 0, s>>>(d, srcBuf);
-        else
-            k_iter_wbal<R, 64, 4><<<(d.n + 61) / 62, 64, 0, s>>>(d, srcBuf);
+    if (lanes == 0 && pipe) {  // warp-balanced contact loop
+        if constexpr (sizeof(R) == 4) {
+            if (threads == 256)
+                k_iter_wbal<R, 256, 4><<<(d.n + 253) / 254, 256, 0, s>>>(d, srcBuf);
+            else
+                k_iter_wbal<R, 128, 6><<<(d.n + 125) / 126, 128, 0, s>>>(d, srcBuf);
+        } else {
+            k_iter_wbal<R, 128, 2><<<(d.n + 125) / 126, 128, 0, s>>>(d, srcBuf);
+        }
     } else if (lanes == 0) {  // block-balanced contact loop
         if constexpr (sizeof(R) == 4) {
             if (threads == 256)
