@@ -325,7 +325,7 @@ yb_status yb_diagnostics(yb_sim* sim, double out[8]);
 yb_status yb_read_state_f64(yb_sim* sim, double* pos, double* vel, double* q);
 
 /* Device-side debugging views used by the parity tests (copies to host buffers):
- *   numCols (n int32), cols (n*128 int32, column-major seg + n*k), stepLimit (n float),
+ *   numCols (n int32), cols (n*128 int32, one row per segment: seg*128 + k), stepLimit (n float),
  *   dx (4n in state precision widened to double).  NULL pointers are skipped. */
 yb_status yb_debug_contacts(yb_sim* sim, int32_t* numCols, int32_t* cols, float* stepLimit);
 yb_status yb_debug_dx(yb_sim* sim, double* dx4);

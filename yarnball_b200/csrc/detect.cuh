@@ -85,11 +85,11 @@ __device__ __forceinline__ R segment_step_limit(const Dev<R>& d, int k, const Sc
     const R safe = E::mul(E::sub(R(1), R(0.1f)), R(0.5f));
     int pen = 0;
     for (int c = 0; c < nc; c++) {
-        const int o = d.cols[k + (size_t)d.n * c];
+        const int o = d.cols[col_at(k, c)];
         const V3<R> b0 = xsub(xyz(d.pos[o]), a0);
         const V3<R> b1 = xsub(xyz(d.pos[o + 1]), a0);
         if (c < RELCAP) {
-            const size_t at = k + (size_t)d.n * c;
+            const size_t at = rel_at(k, c);
             d.relA[at] = v4(b0, b1.x);
             R2<R> rb;
             rb.x = b1.y;

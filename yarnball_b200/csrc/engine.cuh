@@ -12,7 +12,7 @@
 //   vp       VP<R>  {lRest, kStretch, connectionIndex, flags | scene << 8}
 //   stepLim  R      per-segment displacement limit (collision.cu:121-159)
 //   numCols  int    contacts of each segment
-//   cols     int    contact partner ids, column major: cols[seg + n * k], k < MAX_COLS
+//   cols     int    contact partner ids, one row per segment: cols[seg * MAX_COLS + k]
 //   relA/B   V4,R2  partner endpoints relative to p0 for the first RELCAP contacts
 // Segments are the vertices with hasNext; segs[] lists them and is the leaf set of the BVH.
 #pragma once
@@ -57,6 +57,12 @@ struct alignas(sizeof(R) * 2) R2 {
 };
 
 constexpr int RELCAP = 8;  // contacts per segment with staged relative partner positions
+
+// Contact-list addressing: each segment owns a row of MAX_COLS partner ids and a row of RELCAP
+// staged partner positions, so the contacts of one segment are contiguous (the flattened
+// contact loop of the Newton kernel reads consecutive contacts of one owner together).
+__host__ __device__ __forceinline__ size_t col_at(int seg, int c) { return (size_t)seg * MAX_COLS + c; }
+__host__ __device__ __forceinline__ size_t rel_at(int seg, int c) { return (size_t)seg * RELCAP + c; }
 
 template <typename R>
 struct VP {
@@ -125,7 +131,7 @@ struct Dev {
     R* stepLim;
     int* numCols;
     int* cols;
-    V4<R>* relA;      // staged per substep for contacts c < RELCAP, column major [seg + n*c]:
+    V4<R>* relA;      // staged per substep for contacts c < RELCAP, one row per segment [seg*RELCAP + c]:
     R2<R>* relB;      //   relA = (b0 - p0, (b1 - p0).x), relB = (b1 - p0).yz
     int* segs;        // segment -> vertex index, ascending (scene-contiguous)
     const SceneParams<R>* sp;

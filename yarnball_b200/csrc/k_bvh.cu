@@ -263,7 +263,7 @@ constexpr int TRAV_QCAP = 160;      // < 32 left over + up to 4 candidates per l
 template <typename R>
 __device__ __forceinline__ void list_append(const Dev<R>& d, int x, int y) {
     const int pos = atomicAdd(&d.numCols[x], 1);
-    if (pos < MAX_COLS) d.cols[x + (size_t)d.n * pos] = y;
+    if (pos < MAX_COLS) d.cols[col_at(x, pos)] = y;
 }
 
 // Broadphase + narrow phase.  Every segment queries the tree once with its own box (the
@@ -412,16 +412,15 @@ __global__ void __launch_bounds__(128) k_lists(Dev<R> d, int sortLists) {
         if (nc > MAX_COLS) d.err[EW_ERROR] = 1;
         if (nc) atomicMax(&d.err[EW_MAX_COLS], nc);
         nc = min(nc, MAX_COLS);
-        const size_t n = (size_t)d.n;
-        int* __restrict__ cl = d.cols + k;
+        int* __restrict__ cl = d.cols + col_at(k, 0);
         for (int a = 1; a < nc; a++) {
-            const int v = cl[n * a];
+            const int v = cl[a];
             int b = a - 1;
-            while (b >= 0 && cl[n * b] > v) {
-                cl[n * (b + 1)] = cl[n * b];
+            while (b >= 0 && cl[b] > v) {
+                cl[b + 1] = cl[b];
                 b--;
             }
-            cl[n * (b + 1)] = v;
+            cl[b + 1] = v;
         }
         d.numCols[k] = nc;
     }

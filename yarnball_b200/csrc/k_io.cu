@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(256) k_diag(Dev<R> d, double* part) {
             const int nc = d.numCols[i];
             const double twoR = (double)sp.twoR, invb = (double)sp.invb;
             for (int c2 = 0; c2 < nc; c2++) {
-                const int j = d.cols[i + (size_t)d.n * c2];
+                const int j = d.cols[col_at(i, c2)];
                 if (j < i) continue;
                 const V3<double> a0(P.x, P.y, P.z), a1(P1.x, P1.y, P1.z);
                 const V4<R> B0 = d.pos[j], B1 = d.pos[j + 1];

@@ -253,12 +253,12 @@ __global__ void __launch_bounds__(NT, MINB) k_iter(Dev<R> d, int src) {
             // contact's arithmetic, so the dependent partner gather overlaps it (more
             // registers); without it each contact loads then computes.
             const int nc = d.numCols[k];
-            const int* __restrict__ cl = d.cols + k;
+            const int* __restrict__ cl = d.cols + col_at(k, 0);
             const V3<R> e = p1 - p0;
             if constexpr (!PIPE) {
                 for (int c2 = lane; c2 < nc; c2 += T) {
-                    const size_t at = k + (size_t)n * c2;
-                    const int j = __ldg(cl + (size_t)n * c2);
+                    const size_t at = rel_at(k, c2);
+                    const int j = __ldg(cl + c2);
                     V3<R> r0, r1;
                     if (c2 < RELCAP) {
                         const V4<R> A = d.relA[at];
@@ -277,8 +277,8 @@ __global__ void __launch_bounds__(NT, MINB) k_iter(Dev<R> d, int src) {
             V3<R> r0n(R(0)), r1n(R(0));
             D2<R> pdn;
             if (c2 < nc) {
-                const size_t at = k + (size_t)n * c2;
-                const int j = __ldg(cl + (size_t)n * c2);
+                const size_t at = rel_at(k, c2);
+                const int j = __ldg(cl + c2);
                 if (c2 < RELCAP) {
                     const V4<R> A = d.relA[at];
                     const R2<R> Bq = d.relB[at];
@@ -295,8 +295,8 @@ __global__ void __launch_bounds__(NT, MINB) k_iter(Dev<R> d, int src) {
                 const D2<R> pd = pdn;
                 c2 += T;
                 if (c2 < nc) {
-                    const size_t at = k + (size_t)n * c2;
-                    const int j = __ldg(cl + (size_t)n * c2);
+                    const size_t at = rel_at(k, c2);
+                    const int j = __ldg(cl + c2);
                     if (c2 < RELCAP) {
                         const V4<R> A = d.relA[at];
                         const R2<R> Bq = d.relB[at];
@@ -512,8 +512,8 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_bal(Dev<R> d, int src) {
             }
             const int s = lo, c = f - sOff[s];
             const int ks = blockIdx.x * CORE - 1 + s;
-            const size_t at = ks + (size_t)n * c;
-            const int j = __ldg(d.cols + at);
+            const size_t at = rel_at(ks, c);
+            const int j = __ldg(d.cols + col_at(ks, c));
             const V3<R> sp0(sSeg[0][s], sSeg[1][s], sSeg[2][s]);
             V3<R> r0, r1;
             if (c < RELCAP) {
@@ -726,8 +726,8 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_wbal(Dev<R> d, int src) {
             }
             const int s = w0 + lo, c = f - sOffW[wp][lo];
             const int ks = blockIdx.x * CORE - 1 + s;
-            const size_t at = ks + (size_t)n * c;
-            const int j = __ldg(d.cols + at);
+            const size_t at = rel_at(ks, c);
+            const int j = __ldg(d.cols + col_at(ks, c));
             const V3<R> sp0(sSeg[0][s], sSeg[1][s], sSeg[2][s]);
             V3<R> r0, r1;
             if (c < RELCAP) {

@@ -460,10 +460,13 @@ struct Engine : EngineBase {
                 for (int i = 0; i < S->n; i++) maxNc = std::max(maxNc, ((const int32_t*)h.data())[i]);
             if (fwrite(h.data(), 1, a.second, f) != a.second) return YB_ERR_INVALID_ARGUMENT;
         }
-        // cols is column major [k + n * c]: the first maxNc columns hold every listed contact.
+        // cols holds one row of MAX_COLS per segment: the first maxNc entries of every row
+        // hold every listed contact.
         const size_t colBytes = sizeof(int) * (size_t)S->n * (size_t)maxNc;
         std::vector<char> h(colBytes);
-        if (colBytes) YB_CUDA(cudaMemcpy(h.data(), d.cols, colBytes, cudaMemcpyDeviceToHost));
+        if (colBytes)
+            YB_CUDA(cudaMemcpy2D(h.data(), sizeof(int) * maxNc, d.cols, sizeof(int) * MAX_COLS, sizeof(int) * maxNc,
+                                 (size_t)S->n, cudaMemcpyDeviceToHost));
         if (fwrite(&maxNc, 4, 1, f) != 1 || fwrite(h.data(), 1, colBytes, f) != colBytes) return YB_ERR_INVALID_ARGUMENT;
         return YB_OK;
     }
@@ -479,7 +482,9 @@ struct Engine : EngineBase {
         const size_t colBytes = sizeof(int) * (size_t)S->n * (size_t)maxNc;
         std::vector<char> h(colBytes);
         if (fread(h.data(), 1, colBytes, f) != colBytes) return YB_ERR_INVALID_ARGUMENT;
-        if (colBytes) YB_CUDA(cudaMemcpy(d.cols, h.data(), colBytes, cudaMemcpyHostToDevice));
+        if (colBytes)
+            YB_CUDA(cudaMemcpy2D(d.cols, sizeof(int) * MAX_COLS, h.data(), sizeof(int) * maxNc, sizeof(int) * maxNc,
+                                 (size_t)S->n, cudaMemcpyHostToDevice));
         // Host arrays and the segment list from the restored state (not convert_in, which
         // would reset the compensation terms); the BVH is rebuilt by the next detection.
         const yb_status st = download();

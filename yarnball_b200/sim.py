@@ -351,7 +351,8 @@ class Sim:
         sl = np.zeros(n, np.float32)
         check(self._lib.yb_debug_contacts(self._h, ptr(nc, ctypes.c_int32), ptr(cols, ctypes.c_int32),
                                           ptr(sl, ctypes.c_float)), "contacts")
-        lists = [np.sort(cols[i + n * np.arange(nc[i])]) if nc[i] else np.zeros(0, np.int32) for i in range(n)]
+        rows = cols.reshape(n, MAX_COLLISIONS_PER_SEGMENT)
+        lists = [np.sort(rows[i, :nc[i]]) if nc[i] else np.zeros(0, np.int32) for i in range(n)]
         return nc, lists, sl
 
     def debug_dx(self):
