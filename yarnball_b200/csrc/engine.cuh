@@ -115,6 +115,14 @@ struct alignas(16) WNode {
     int last[4];
 };
 
+// Query record of a sorted leaf, written by the refit for the traversal: the segment's padded
+// box, the segment and its scene (one coalesced load when a lane starts a query).
+template <typename R>
+struct alignas(16) QRec {
+    R mn[3], mx[3];
+    int k, sc;
+};
+
 template <typename R>
 struct Dev {
     int n;            // vertices
@@ -139,6 +147,7 @@ struct Dev {
     // BVH
     BNode<R>* nodes;  // nseg - 1 internal nodes
     WNode<R>* wide;   // nseg - 1 wide nodes (rebuilt after every refit)
+    QRec<R>* qrec;    // per sorted leaf: box, segment, scene (written by the refit)
     int* nodeLast;    // sorted position of the last leaf of each internal node's range
     int* leafParent;  // per sorted leaf position
     unsigned* refitCount;

@@ -177,8 +177,20 @@ __global__ void __launch_bounds__(256) k_refit(Dev<R> d, const int* __restrict__
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= d.nseg) return;
     const int k = sortedVals[p];
-    const SceneParams<R>& sp = d.sp[scene_of(d.vp[k].flags)];
+    const int sc = scene_of(d.vp[k].flags);
+    const SceneParams<R>& sp = d.sp[sc];
     Box<R> b = segment_box(d, k, sp);
+    {
+        QRec<R> r;
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            r.mn[a] = b.mn[a];
+            r.mx[a] = b.mx[a];
+        }
+        r.k = k;
+        r.sc = sc;
+        d.qrec[p] = r;
+    }
     int code = -(k + 1);
     if (d.nseg == 1) return;
     int node = d.leafParent[p];
@@ -317,9 +329,22 @@ __global__ void __launch_bounds__(TRAV_THREADS) k_traverse(Dev<R> d) {
             if (!walking) {
                 qi = base + __popc(idle & lt);
                 if (qi < nseg) {
-                    k = d.vals[0][qi];
-                    const int sc = scene_of(d.vp[k].flags);
-                    qb = segment_box(d, k, d.sp[sc]);
+                    QRec<R> r;
+                    if constexpr (sizeof(R) == 4) {
+                        const float4* src = reinterpret_cast<const float4*>(d.qrec + qi);
+                        float4* dst = reinterpret_cast<float4*>(&r);
+                        dst[0] = __ldg(src);
+                        dst[1] = __ldg(src + 1);
+                    } else {
+                        r = d.qrec[qi];
+                    }
+                    k = r.k;
+                    const int sc = r.sc;
+#pragma unroll
+                    for (int a = 0; a < 3; a++) {
+                        qb.mn[a] = r.mn[a];
+                        qb.mx[a] = r.mx[a];
+                    }
                     node = d.sceneRoot[sc];
                     top = 0;
                     steps = 0;
@@ -453,8 +478,8 @@ void launch_bvh_reset(const Dev<R>& d, cudaStream_t s) {
 
 template <typename R>
 void launch_bvh_refit(const Dev<R>& d, cudaStream_t s) {
-    if (d.nseg <= 1) return;
-    cudaMemsetAsync(d.refitCount, 0, sizeof(unsigned) * (d.nseg - 1), s);
+    if (d.nseg <= 0) return;  // one segment: no internal node, but its query record is written
+    if (d.nseg > 1) cudaMemsetAsync(d.refitCount, 0, sizeof(unsigned) * (d.nseg - 1), s);
     k_refit<R><<<(d.nseg + 255) / 256, 256, 0, s>>>(d, d.vals[0]);
     k_widen<R><<<(d.nseg - 1 + 255) / 256, 256, 0, s>>>(d);
 }

@@ -418,68 +418,33 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_bal(Dev<R> d, int src) {
     __shared__ int sScene[B];
     __shared__ int sWarp[NW];
 
+    // The contact loop runs first and accumulates from zero; the vertex's own terms (inertia,
+    // glue, stretch) are loaded and added after it, so their inputs are not live (in
+    // registers) across the loop.
     V3<R> fa(R(0)), fb(R(0));
     H3<R> Ha, Hb;
     Ha.zero(); Hb.zero();
-    R sl = yinf<R>();
-    uint32_t flags = 0;
-    R invMass = R(0), lRest = R(1), kStretch = R(0);
-    V3<R> p0(R(0)), p1(R(0)), dx(R(0)), dx1(R(0));
-    Q<R> q0 = qmk(R(0), R(0), R(0), R(1));
-    const SceneParams<R>* spp = d.sp;
     int nc = 0, sc = 0;
-
-    if (valid) {
-        const VP<R> vp = d.vp[k];
-        flags = vp.flags;
-        lRest = vp.lRest;
-        kStretch = vp.kStretch;
-        sc = scene_of(flags);
-        spp = &d.sp[sc];
-        const SceneParams<R>& sp = *spp;
-        const V4<R> P = d.pos[k];
-        p0 = xyz(P);
-        invMass = P.w;
-        const D2<R> own = DX[k];
-        dx = xyz(own.a);
-        dx1 = xyz(own.b);
-        q0 = qof(QO[k]);
-        const R D = sp.D;
-        if (invMass != R(0)) {
-            const V4<R> v = d.vel[k];
-            const R hh = sp.hh;
-            const V3<R> y(sp.h * v.x + hh * sp.gx, sp.h * v.y + hh * sp.gy, sp.h * v.z + hh * sp.gz);
-            Ha.diag(R(1) / (invMass * hh));
-            fa = (R(1) / (hh * invMass)) * (y - dx);
+    {
+        V3<R> p0(R(0)), e(R(0)), dx(R(0)), dx1(R(0));
+        if (valid) {
+            const uint32_t fl = d.vp[k].flags;
+            sc = scene_of(fl);
+            const D2<R> own = DX[k];
+            dx = xyz(own.a);
+            dx1 = xyz(own.b);
+            p0 = xyz(d.pos[k]);
+            if (fl & F_HAS_NEXT) {
+                e = xyz(d.pos[k + 1]) - p0;
+                nc = d.numCols[k];
+            }
         }
-        if (vp.cid >= 0) {
-            const R stiff = R(40);
-            const V3<R> pc = xyz(d.pos[vp.cid]);
-            const V3<R> dc = xyz(DX[vp.cid].a);
-            fa -= stiff * ((p0 - pc) + (dx - dc) + D * dx);
-            Ha.add_diag(stiff * (R(1) + D));
-        }
-        if (flags & F_HAS_NEXT) {
-            p1 = xyz(d.pos[k + 1]);
-            sl = d.stepLim[k];
-            nc = d.numCols[k];
-            const R invl = R(1) / lRest;
-            const V3<R> c = ((p1 - p0) + (dx1 - dx)) * invl - qrotate(q0, V3<R>(R(1), R(0), R(0)));
-            const R ks = kStretch * invl;
-            R dd = ks * invl;
-            fa += ks * c - (D * dd) * dx;
-            fb += -ks * c - (D * dd) * dx1;
-            dd *= R(1) + D;
-            Ha.add_diag(dd);
-            Hb.add_diag(dd);
-        }
+        sSeg[0][t] = p0.x; sSeg[1][t] = p0.y; sSeg[2][t] = p0.z;
+        sSeg[3][t] = e.x; sSeg[4][t] = e.y; sSeg[5][t] = e.z;
+        sSeg[6][t] = dx.x; sSeg[7][t] = dx.y; sSeg[8][t] = dx.z;
+        sSeg[9][t] = dx1.x; sSeg[10][t] = dx1.y; sSeg[11][t] = dx1.z;
+        sScene[t] = sc;
     }
-    const V3<R> e = p1 - p0;
-    sSeg[0][t] = p0.x; sSeg[1][t] = p0.y; sSeg[2][t] = p0.z;
-    sSeg[3][t] = e.x; sSeg[4][t] = e.y; sSeg[5][t] = e.z;
-    sSeg[6][t] = dx.x; sSeg[7][t] = dx.y; sSeg[8][t] = dx.z;
-    sSeg[9][t] = dx1.x; sSeg[10][t] = dx1.y; sSeg[11][t] = dx1.z;
-    sScene[t] = sc;
     // block exclusive scan of the contact counts
     {
         const int lane = t & 31, w = t >> 5;
@@ -553,6 +518,54 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_bal(Dev<R> d, int src) {
         __syncthreads();
     }
 
+    // the vertex's own terms (cosserat.cu:40-81)
+    R sl = yinf<R>();
+    uint32_t flags = 0;
+    R invMass = R(0), lRest = R(1), kStretch = R(0);
+    const V3<R> p0(sSeg[0][t], sSeg[1][t], sSeg[2][t]);
+    const V3<R> e(sSeg[3][t], sSeg[4][t], sSeg[5][t]);
+    const V3<R> dx(sSeg[6][t], sSeg[7][t], sSeg[8][t]);
+    Q<R> q0 = qmk(R(0), R(0), R(0), R(1));
+    const SceneParams<R>* spp = d.sp;
+    if (valid) {
+        const VP<R> vp = d.vp[k];
+        flags = vp.flags;
+        lRest = vp.lRest;
+        kStretch = vp.kStretch;
+        spp = &d.sp[sc];
+        const SceneParams<R>& sp = *spp;
+        invMass = d.pos[k].w;
+        q0 = qof(QO[k]);
+        const R D = sp.D;
+        if (invMass != R(0)) {
+            const V4<R> v = d.vel[k];
+            const R hh = sp.hh;
+            const V3<R> y(sp.h * v.x + hh * sp.gx, sp.h * v.y + hh * sp.gy, sp.h * v.z + hh * sp.gz);
+            Ha.add_diag(R(1) / (invMass * hh));
+            fa += (R(1) / (hh * invMass)) * (y - dx);
+        }
+        if (vp.cid >= 0) {
+            const R stiff = R(40);
+            const V3<R> pc = xyz(d.pos[vp.cid]);
+            const V3<R> dc = xyz(DX[vp.cid].a);
+            fa -= stiff * ((p0 - pc) + (dx - dc) + D * dx);
+            Ha.add_diag(stiff * (R(1) + D));
+        }
+        if (flags & F_HAS_NEXT) {
+            const V3<R> dx1(sSeg[9][t], sSeg[10][t], sSeg[11][t]);
+            sl = d.stepLim[k];
+            const R invl = R(1) / lRest;
+            const V3<R> c = (e + (dx1 - dx)) * invl - qrotate(q0, V3<R>(R(1), R(0), R(0)));
+            const R ks = kStretch * invl;
+            R dd = ks * invl;
+            fa += ks * c - (D * dd) * dx;
+            fb += -ks * c - (D * dd) * dx1;
+            dd *= R(1) + D;
+            Ha.add_diag(dd);
+            Hb.add_diag(dd);
+        }
+    }
+
     sFb[0][t] = fb.x; sFb[1][t] = fb.y; sFb[2][t] = fb.z;
 #pragma unroll
     for (int q = 0; q < 6; q++) sHb[q][t] = Hb.d[q];
@@ -587,7 +600,7 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_bal(Dev<R> d, int src) {
         d.dx[src ^ 1][k] = o;
         Q<R> qn = q0;
         if (!(flags & F_FIX_ORI) && (flags & F_HAS_NEXT)) {
-            V3<R> v = ((p1 - p0) + (dxb - dxn)) * (R(1) / lRest);
+            V3<R> v = (e + (dxb - dxn)) * (R(1) / lRest);
             v *= R(-2) * kStretch;
             Q<R> b = qmk(R(0), R(0), R(0), R(0));
             if (flags & F_HAS_PREV) {

@@ -343,6 +343,7 @@ struct Engine : EngineBase {
         want((void**)&d.err, sizeof(int) * EW_COUNT);
         want((void**)&d.nodes, sizeof(BNode<R>) * nn);
         want((void**)&d.wide, sizeof(WNode<R>) * nn);
+        want((void**)&d.qrec, sizeof(QRec<R>) * n);
         want((void**)&d.nodeLast, sizeof(int) * nn);
         want((void**)&d.leafParent, sizeof(int) * n);
         want((void**)&d.refitCount, sizeof(unsigned) * nn);
@@ -646,10 +647,10 @@ struct Engine : EngineBase {
             if (rebuild) {
                 launch_bvh_rebuild(d, st, sortScratch, sortBytes, keyBits);
                 const int passes = d.nseg > 1 ? (keyBits + 7) / 8 : 0;
-                k += 3 + (d.nseg > 1 ? 2 + passes : 0) + 1 + (d.nseg > 1 ? 1 : 0);
+                k += 3 + (d.nseg > 1 ? 2 + passes : 0) + 1 + 1;
             } else {
                 launch_bvh_refit(d, st);
-                k += d.nseg > 1 ? 1 : 0;
+                k += 1;
             }
             launch_traverse(d, st); k += 2;
         } else {
@@ -819,11 +820,11 @@ struct Engine : EngineBase {
                 mark(1);
                 launch_bvh_rebuild(d, st, sortScratch, sortBytes, keyBits);
                 const int passes = d.nseg > 1 ? (keyBits + 7) / 8 : 0;
-                launches[1] += 3 + (d.nseg > 1 ? 2 + passes : 0) + 1 + (d.nseg > 1 ? 1 : 0);
+                launches[1] += 3 + (d.nseg > 1 ? 2 + passes : 0) + 1 + 1;
             } else {
                 mark(2);
                 launch_bvh_refit(d, st);
-                launches[2] += d.nseg > 1 ? 1 : 0;
+                launches[2] += 1;
             }
             mark(3);
             launch_traverse(d, st); launches[3] += 2;
