@@ -179,7 +179,7 @@ const char* yb_status_string(yb_status s);
 /* Engine tuning of the Newton kernel: threads per block, lanes per vertex (lanes split a
  * segment's contact loop; 0 selects a load-balanced kernel that flattens contact lists) and
  * software pipelining of the contact loop (with lanes 0: flatten per warp instead of per
- * block); valid shapes: (128|256, 0, 0|1), (128|256, 1, 0|1), (256, 2, 0), (256, 4, 0|1),
+ * block); valid shapes: (128, 0, 0|1), (128|256, 1, 0|1), (256, 2, 0), (256, 4, 0|1),
  * (512, 4, 0), (256|512, 8, 0).  useGraphs: replay captured CUDA graphs per substep.
  * Default (256, 4, 0), graphs on. */
 yb_status yb_set_tuning(yb_sim* sim, int32_t iterThreads, int32_t lanesPerVertex, int32_t pipelined,

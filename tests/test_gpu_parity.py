@@ -148,8 +148,7 @@ def test_dense_pile_substep_vs_fp64():
 
 
 SHAPES = [(256, 1, False), (128, 1, False), (256, 2, False), (256, 4, False), (512, 4, False), (256, 8, False),
-          (512, 8, False), (128, 1, True), (256, 1, True), (256, 4, True), (256, 0, False), (128, 0, False),
-          (256, 0, True), (128, 0, True)]
+          (512, 8, False), (128, 1, True), (256, 1, True), (256, 4, True), (128, 0, False), (128, 0, True)]
 
 
 @pytest.mark.parametrize("shape", SHAPES)

@@ -413,7 +413,8 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_bal(Dev<R> d, int src) {
     __shared__ R sSL[B];
     __shared__ R sDX[3][B];
     __shared__ R sSeg[12][B];  // p0, e = p1 - p0, dx, dx1 of each slot's segment
-    __shared__ R sCon[18][B];  // contributions of one chunk of contacts
+    __shared__ R sCon[2][18][B];  // contributions of one chunk of contacts (double buffered)
+    __shared__ int sOwn[2][B];     // owning slot of each contact of a chunk (double buffered)
     __shared__ int sOff[B + 1];
     __shared__ int sScene[B];
     __shared__ int sWarp[NW];
@@ -464,18 +465,26 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_bal(Dev<R> d, int src) {
     }
     const int total = sOff[B];
     const int myOff = sOff[t];
-    for (int base = 0; base < total; base += NT) {
+    // Chunks of NT contacts, one per thread.  Each thread writes its own slot index over its
+    // contacts of the next chunk before the current chunk's barrier, which publishes it, and
+    // the contributions are double buffered: a buffer is written again only after the next
+    // chunk's barrier, which every thread reaches after summing it, so each chunk needs one
+    // barrier.
+    for (int g = myOff; g < min(myOff + nc, NT); g++) sOwn[0][g] = t;
+    __syncthreads();
+    int buf = 0;
+    for (int base = 0; base < total; base += NT, buf ^= 1) {
         const int f = base + t;
+        {
+            const int nb = base + NT;
+            const int g1 = min(myOff + nc, nb + NT);
+            for (int g = max(myOff, nb); g < g1; g++) sOwn[buf ^ 1][g - nb] = t;
+        }
         V3<R> cfa(R(0)), cfb(R(0));
         H3<R> cHa, cHb;
         cHa.zero(); cHb.zero();
         if (f < total) {
-            int lo = 0, hi = B - 1;  // owner: the last slot whose offset is <= f
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (sOff[mid] <= f) lo = mid; else hi = mid - 1;
-            }
-            const int s = lo, c = f - sOff[s];
+            const int s = sOwn[buf][t], c = f - sOff[s];
             const int ks = blockIdx.x * CORE - 1 + s;
             const size_t at = rel_at(ks, c);
             const int j = __ldg(d.cols + col_at(ks, c));
@@ -496,26 +505,26 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_bal(Dev<R> d, int src) {
             const V3<R> sdx1(sSeg[9][s], sSeg[10][s], sSeg[11][s]);
             contact_term(se, sdx, sdx1, r0, r1, xyz(pd.a), xyz(pd.b), d.sp[sScene[s]], cfa, cHa, cfb, cHb);
         }
-        sCon[0][t] = cfa.x; sCon[1][t] = cfa.y; sCon[2][t] = cfa.z;
-        sCon[3][t] = cfb.x; sCon[4][t] = cfb.y; sCon[5][t] = cfb.z;
+        R (*con)[B] = sCon[buf];
+        con[0][t] = cfa.x; con[1][t] = cfa.y; con[2][t] = cfa.z;
+        con[3][t] = cfb.x; con[4][t] = cfb.y; con[5][t] = cfb.z;
 #pragma unroll
         for (int q = 0; q < 6; q++) {
-            sCon[6 + q][t] = cHa.d[q];
-            sCon[12 + q][t] = cHb.d[q];
+            con[6 + q][t] = cHa.d[q];
+            con[12 + q][t] = cHb.d[q];
         }
         __syncthreads();
         const int f0 = max(myOff, base), f1 = min(myOff + nc, base + NT);
         for (int g = f0; g < f1; g++) {
             const int i = g - base;
-            fa += V3<R>(sCon[0][i], sCon[1][i], sCon[2][i]);
-            fb += V3<R>(sCon[3][i], sCon[4][i], sCon[5][i]);
+            fa += V3<R>(con[0][i], con[1][i], con[2][i]);
+            fb += V3<R>(con[3][i], con[4][i], con[5][i]);
 #pragma unroll
             for (int q = 0; q < 6; q++) {
-                Ha.d[q] += sCon[6 + q][i];
-                Hb.d[q] += sCon[12 + q][i];
+                Ha.d[q] += con[6 + q][i];
+                Hb.d[q] += con[12 + q][i];
             }
         }
-        __syncthreads();
     }
 
     // the vertex's own terms (cosserat.cu:40-81)
@@ -651,68 +660,32 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_wbal(Dev<R> d, int src) {
     __shared__ int sOffW[NW][33];
     __shared__ int sScene[B];
 
+    // The contact loop runs first and accumulates from zero; the vertex's own terms are
+    // loaded and added after it (their inputs are not live across the loop).
     V3<R> fa(R(0)), fb(R(0));
     H3<R> Ha, Hb;
     Ha.zero(); Hb.zero();
-    R sl = yinf<R>();
-    uint32_t flags = 0;
-    R invMass = R(0), lRest = R(1), kStretch = R(0);
-    V3<R> p0(R(0)), p1(R(0)), dx(R(0)), dx1(R(0));
-    Q<R> q0 = qmk(R(0), R(0), R(0), R(1));
-    const SceneParams<R>* spp = d.sp;
     int nc = 0, sc = 0;
-
-    if (valid) {
-        const VP<R> vp = d.vp[k];
-        flags = vp.flags;
-        lRest = vp.lRest;
-        kStretch = vp.kStretch;
-        sc = scene_of(flags);
-        spp = &d.sp[sc];
-        const SceneParams<R>& sp = *spp;
-        const V4<R> P = d.pos[k];
-        p0 = xyz(P);
-        invMass = P.w;
-        const D2<R> own = DX[k];
-        dx = xyz(own.a);
-        dx1 = xyz(own.b);
-        q0 = qof(QO[k]);
-        const R D = sp.D;
-        if (invMass != R(0)) {
-            const V4<R> v = d.vel[k];
-            const R hh = sp.hh;
-            const V3<R> y(sp.h * v.x + hh * sp.gx, sp.h * v.y + hh * sp.gy, sp.h * v.z + hh * sp.gz);
-            Ha.diag(R(1) / (invMass * hh));
-            fa = (R(1) / (hh * invMass)) * (y - dx);
+    {
+        V3<R> p0(R(0)), e(R(0)), dx(R(0)), dx1(R(0));
+        if (valid) {
+            const uint32_t fl = d.vp[k].flags;
+            sc = scene_of(fl);
+            const D2<R> own = DX[k];
+            dx = xyz(own.a);
+            dx1 = xyz(own.b);
+            p0 = xyz(d.pos[k]);
+            if (fl & F_HAS_NEXT) {
+                e = xyz(d.pos[k + 1]) - p0;
+                nc = d.numCols[k];
+            }
         }
-        if (vp.cid >= 0) {
-            const R stiff = R(40);
-            const V3<R> pc = xyz(d.pos[vp.cid]);
-            const V3<R> dc = xyz(DX[vp.cid].a);
-            fa -= stiff * ((p0 - pc) + (dx - dc) + D * dx);
-            Ha.add_diag(stiff * (R(1) + D));
-        }
-        if (flags & F_HAS_NEXT) {
-            p1 = xyz(d.pos[k + 1]);
-            sl = d.stepLim[k];
-            nc = d.numCols[k];
-            const R invl = R(1) / lRest;
-            const V3<R> c = ((p1 - p0) + (dx1 - dx)) * invl - qrotate(q0, V3<R>(R(1), R(0), R(0)));
-            const R ks = kStretch * invl;
-            R dd = ks * invl;
-            fa += ks * c - (D * dd) * dx;
-            fb += -ks * c - (D * dd) * dx1;
-            dd *= R(1) + D;
-            Ha.add_diag(dd);
-            Hb.add_diag(dd);
-        }
+        sSeg[0][t] = p0.x; sSeg[1][t] = p0.y; sSeg[2][t] = p0.z;
+        sSeg[3][t] = e.x; sSeg[4][t] = e.y; sSeg[5][t] = e.z;
+        sSeg[6][t] = dx.x; sSeg[7][t] = dx.y; sSeg[8][t] = dx.z;
+        sSeg[9][t] = dx1.x; sSeg[10][t] = dx1.y; sSeg[11][t] = dx1.z;
+        sScene[t] = sc;
     }
-    const V3<R> e = p1 - p0;
-    sSeg[0][t] = p0.x; sSeg[1][t] = p0.y; sSeg[2][t] = p0.z;
-    sSeg[3][t] = e.x; sSeg[4][t] = e.y; sSeg[5][t] = e.z;
-    sSeg[6][t] = dx.x; sSeg[7][t] = dx.y; sSeg[8][t] = dx.z;
-    sSeg[9][t] = dx1.x; sSeg[10][t] = dx1.y; sSeg[11][t] = dx1.z;
-    sScene[t] = sc;
     // warp exclusive scan of the contact counts: each warp flattens its own 32 vertices
     const int lane = t & 31, wp = t >> 5, w0 = wp << 5;
     int incl = nc;
@@ -780,6 +753,54 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_wbal(Dev<R> d, int src) {
         __syncwarp();
     }
 
+    // the vertex's own terms (cosserat.cu:40-81)
+    R sl = yinf<R>();
+    uint32_t flags = 0;
+    R invMass = R(0), lRest = R(1), kStretch = R(0);
+    const V3<R> p0(sSeg[0][t], sSeg[1][t], sSeg[2][t]);
+    const V3<R> e(sSeg[3][t], sSeg[4][t], sSeg[5][t]);
+    const V3<R> dx(sSeg[6][t], sSeg[7][t], sSeg[8][t]);
+    Q<R> q0 = qmk(R(0), R(0), R(0), R(1));
+    const SceneParams<R>* spp = d.sp;
+    if (valid) {
+        const VP<R> vp = d.vp[k];
+        flags = vp.flags;
+        lRest = vp.lRest;
+        kStretch = vp.kStretch;
+        spp = &d.sp[sc];
+        const SceneParams<R>& sp = *spp;
+        invMass = d.pos[k].w;
+        q0 = qof(QO[k]);
+        const R D = sp.D;
+        if (invMass != R(0)) {
+            const V4<R> v = d.vel[k];
+            const R hh = sp.hh;
+            const V3<R> y(sp.h * v.x + hh * sp.gx, sp.h * v.y + hh * sp.gy, sp.h * v.z + hh * sp.gz);
+            Ha.add_diag(R(1) / (invMass * hh));
+            fa += (R(1) / (hh * invMass)) * (y - dx);
+        }
+        if (vp.cid >= 0) {
+            const R stiff = R(40);
+            const V3<R> pc = xyz(d.pos[vp.cid]);
+            const V3<R> dc = xyz(DX[vp.cid].a);
+            fa -= stiff * ((p0 - pc) + (dx - dc) + D * dx);
+            Ha.add_diag(stiff * (R(1) + D));
+        }
+        if (flags & F_HAS_NEXT) {
+            const V3<R> dx1(sSeg[9][t], sSeg[10][t], sSeg[11][t]);
+            sl = d.stepLim[k];
+            const R invl = R(1) / lRest;
+            const V3<R> c = (e + (dx1 - dx)) * invl - qrotate(q0, V3<R>(R(1), R(0), R(0)));
+            const R ks = kStretch * invl;
+            R dd = ks * invl;
+            fa += ks * c - (D * dd) * dx;
+            fb += -ks * c - (D * dd) * dx1;
+            dd *= R(1) + D;
+            Ha.add_diag(dd);
+            Hb.add_diag(dd);
+        }
+    }
+
     sFb[0][t] = fb.x; sFb[1][t] = fb.y; sFb[2][t] = fb.z;
 #pragma unroll
     for (int q = 0; q < 6; q++) sHb[q][t] = Hb.d[q];
@@ -814,7 +835,7 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_wbal(Dev<R> d, int src) {
         d.dx[src ^ 1][k] = o;
         Q<R> qn = q0;
         if (!(flags & F_FIX_ORI) && (flags & F_HAS_NEXT)) {
-            V3<R> v = ((p1 - p0) + (dxb - dxn)) * (R(1) / lRest);
+            V3<R> v = (e + (dxb - dxn)) * (R(1) / lRest);
             v *= R(-2) * kStretch;
             Q<R> b = qmk(R(0), R(0), R(0), R(0));
             if (flags & F_HAS_PREV) {
@@ -862,23 +883,15 @@ void launch_iter(const Dev<R>& d, int srcBuf, int threads, int lanes, int pipe, 
 #define YB_ITER(NT, T, MINB, P) \
     k_iter<R, NT, T, MINB, P><<<(d.n + (NT / T) - 3) / ((NT / T) - 2), NT, 0, s>>>(d, srcBuf)
     if (lanes == 0 && pipe) {  // warp-balanced contact loop
-        if constexpr (sizeof(R) == 4) {
-            if (threads == 256)
-                k_iter_wbal<R, 256, 4><<<(d.n + 253) / 254, 256, 0, s>>>(d, srcBuf);
-            else
-                k_iter_wbal<R, 128, 6><<<(d.n + 125) / 126, 128, 0, s>>>(d, srcBuf);
-        } else {
-            k_iter_wbal<R, 128, 2><<<(d.n + 125) / 126, 128, 0, s>>>(d, srcBuf);
-        }
-    } else if (lanes == 0) {  // block-balanced contact loop
-        if constexpr (sizeof(R) == 4) {
-            if (threads == 256)
-                k_iter_bal<R, 256, 4><<<(d.n + 253) / 254, 256, 0, s>>>(d, srcBuf);
-            else
-                k_iter_bal<R, 128, 6><<<(d.n + 125) / 126, 128, 0, s>>>(d, srcBuf);
-        } else {
-            k_iter_bal<R, 128, 2><<<(d.n + 125) / 126, 128, 0, s>>>(d, srcBuf);
-        }
+        if constexpr (sizeof(R) == 4)
+            k_iter_wbal<R, 128, 6><<<(d.n + 125) / 126, 128, 0, s>>>(d, srcBuf);
+        else
+            k_iter_wbal<R, 64, 4><<<(d.n + 61) / 62, 64, 0, s>>>(d, srcBuf);
+    } else if (lanes == 0) {  // block-balanced contact loop (shared memory bounds the block size)
+        if constexpr (sizeof(R) == 4)
+            k_iter_bal<R, 128, 6><<<(d.n + 125) / 126, 128, 0, s>>>(d, srcBuf);
+        else
+            k_iter_bal<R, 64, 4><<<(d.n + 61) / 62, 64, 0, s>>>(d, srcBuf);
     } else if (pipe) {
         if (lanes == 4) YB_ITER(256, 4, 2, true);
         else if (threads == 128) YB_ITER(128, 1, 4, true);

@@ -1225,7 +1225,7 @@ const char* yb_status_string(yb_status s) {
 }
 
 static bool valid_shape(int threads, int lanes, int pipe) {
-    if (lanes == 0) return threads == 128 || threads == 256;
+    if (lanes == 0) return threads == 128;
     if (pipe) return (lanes == 1 && (threads == 128 || threads == 256)) || (lanes == 4 && threads == 256);
     return (lanes == 1 && (threads == 128 || threads == 256)) || (lanes == 2 && threads == 256) ||
            ((lanes == 4 || lanes == 8) && (threads == 256 || threads == 512));
@@ -1255,8 +1255,7 @@ yb_status yb_autotune(yb_sim* S, int32_t* bestThreads, int32_t* bestLanes, int32
     if (!S) return YB_ERR_INVALID_ARGUMENT;
     if (!S->configured) return YB_ERR_NOT_CONFIGURED;
     static const int shapes[][3] = {{256, 1, 0}, {128, 1, 0}, {256, 2, 0}, {256, 4, 0}, {512, 4, 0}, {256, 8, 0},
-                                    {512, 8, 0}, {128, 1, 1}, {256, 1, 1}, {256, 4, 1}, {256, 0, 0}, {128, 0, 0},
-                                    {256, 0, 1}, {128, 0, 1}};
+                                    {512, 8, 0}, {128, 1, 1}, {256, 1, 1}, {256, 4, 1}, {128, 0, 0}, {128, 0, 1}};
     float best = INFINITY;
     int bt = S->iterThreads, bl = S->iterLanes, bp = S->iterPipe;
     S->eng->write_params();
