@@ -268,7 +268,6 @@ __global__ void __launch_bounds__(256) k_widen(Dev<R> d) {
 constexpr int BVH_STACK = 96;
 constexpr int TRAV_THREADS = 128;
 constexpr int TRAV_WARPS = TRAV_THREADS / 32;
-constexpr int TRAV_MINB = 10;      // resident blocks per SM: the walk is bound by load latency
 constexpr int TRAV_QCAP = 160;      // < 32 left over + up to 4 candidates per lane
 
 // Appends y to x's contact list.  The count keeps growing past MAX_COLS so that the list
@@ -305,7 +304,7 @@ __device__ __forceinline__ void trav_load_wide(const WNode<R>* wide, int node, W
 }
 
 template <typename R>
-__global__ void __launch_bounds__(TRAV_THREADS, TRAV_MINB) k_traverse(Dev<R> d) {
+__global__ void __launch_bounds__(TRAV_THREADS) k_traverse(Dev<R> d) {
     __shared__ int sQx[TRAV_WARPS][TRAV_QCAP];
     __shared__ int sQy[TRAV_WARPS][TRAV_QCAP];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;

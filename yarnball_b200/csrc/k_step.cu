@@ -100,6 +100,11 @@ __global__ void __launch_bounds__(256) k_end(Dev<R> d, int fb, int copyQ, int ka
 // IPC log barrier E(d) = -kCollision (d-1)^2 ln d on the normalised gap d, clamped to 1e-3:
 // returns dH = E''(d) / b^2 and the force magnitude ff (cosserat.cu:114-125).  Below d=1e-2
 // the log and the reciprocals are evaluated in FP64.
+// Hint: bring the line holding p into L1 (no register is held until the data is used).
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
 template <typename R>
 __device__ __forceinline__ void barrier_terms(R d, R kCol, R invb, R& dH, R& ff) {
     if (sizeof(R) == 4 && d < R(1e-2)) {
@@ -429,6 +434,11 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_bal(Dev<R> d, int src) {
     {
         V3<R> p0(R(0)), e(R(0)), dx(R(0)), dx1(R(0));
         if (valid) {
+            // inputs of the vertex's own terms, used after the contact loop
+            prefetch_l1(d.vel + k);
+            prefetch_l1(QO + k);
+            prefetch_l1(d.qRest + k);
+            prefetch_l1(d.stepLim + k);
             const uint32_t fl = d.vp[k].flags;
             sc = scene_of(fl);
             const D2<R> own = DX[k];
