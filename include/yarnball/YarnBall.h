@@ -9,7 +9,7 @@
 //   * advance() returns dt (the reference declares float but returns nothing);
 //   * when <glm/glm.hpp> is available vec3/vec4 are glm's, otherwise minimal POD structs
 //     with the same layout; Rotor is a POD {x, y, z, w} (w scalar), like Kit::Rotor's layout;
-//   * rendering and the fibre mesher are not part of this library; the file readers and
+//   * rendering is not part of this library; the file readers and
 //     buildFromJSON are free functions here, as in the reference (YarnBall.h:208-211).
 #pragma once
 #include <cstdint>
@@ -215,6 +215,13 @@ class Sim {
     void exportToOBJ(std::string path) {
         push();
         report_file(yb_export_obj(h_, path.c_str()));
+    }
+    // io/fiberMesher.cpp:9-157; throws like the reference when the file cannot be opened.
+    void exportFiberMesh(std::string path) {
+        push();
+        const yb_status st = yb_export_fiber_mesh(h_, path.c_str());
+        if (st == YB_ERR_IO) throw std::runtime_error("Failed to open file for writing");
+        check(st);
     }
 
     // Sim::glueEndpoints (io/jsonBuilder.cpp:174-212), on the host arrays.

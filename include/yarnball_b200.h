@@ -249,6 +249,16 @@ yb_status yb_export_bcc(yb_sim* sim, const char* path, int32_t asPolyline);
  * decimals and one "l i j ..." polyline (1-based) per curve. */
 yb_status yb_export_obj(yb_sim* sim, const char* path);
 
+/* Sim::exportFiberMesh (io/fiberMesher.cpp:9-157): download(), then every segment as 8 twisted
+ * fibres (Catmull-Rom centre line, frame blended between neighbouring rotors, random frizz)
+ * and random fuzz strands, written as OBJ polylines ("o fiber", "o fuzz").  The random stream
+ * is the reference's (xoroshiro128+, seed 0x12345678, the same draws in the same order, the
+ * three draws of one vector taken x, y, z), so vertex and line counts and indices match it;
+ * vertex positions are evaluated on the GPU and agree to float rounding.  Uses meta of scene 0
+ * for the yarn radius.  An unopenable path gives YB_ERR_IO ("Failed to open file for
+ * writing" in yb_last_io_error). */
+yb_status yb_export_fiber_mesh(yb_sim* sim, const char* path);
+
 /* Full-state checkpoint (no reference counterpart; the exporters above keep positions only).
  * Writes the device state in the simulation's precision (positions with their compensation
  * terms, velocities, last velocities, rotors, rest rotors, per-vertex constants, the contact

@@ -78,3 +78,15 @@ def test_file_entry_points_validate_arguments_on_cpu():
     out = ctypes.c_void_p()
     assert lib.yb_load_state(b"/nonexistent-dir/x.ybck", ctypes.byref(out)) != 0
     assert not out.value
+
+
+def test_mesher_stream_known_answers():
+    from oracle import mesher
+    assert mesher.splitmix64(0) == 0xE220A8397B1DCDAF  # SplitMix64's published first output for seed 0
+    a, b = mesher.Xoroshiro128p(0x12345678), mesher.Xoroshiro128p(0x12345678)
+    xs = [a.uniform() for _ in range(1000)]
+    assert xs == [b.uniform() for _ in range(1000)]
+    assert all(0.0 <= x <= 1.0 for x in xs) and 0.45 < sum(xs) / len(xs) < 0.55
+    r = mesher.Xoroshiro128p(1)
+    s0, s1 = r.s0, r.s1
+    assert r.next() == (s0 + s1) & mesher.M64

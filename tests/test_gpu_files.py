@@ -119,3 +119,26 @@ def test_load_state_rejects_a_foreign_file(tmp_path):
     p.write_bytes(b"not a checkpoint at all")
     with pytest.raises(RuntimeError):
         Sim.load_state(str(p))
+
+
+def test_export_fiber_mesh_matches_restatement(tmp_path):
+    from oracle import mesher
+    sim = scenes.build_readme()
+    sim.advance(1 / 30)
+    path = tmp_path / "fibers.obj"
+    sim.exportFiberMesh(str(path))
+    got = mesher.parse_obj(path.read_text())
+    m = sim.meta
+    fv, fl, zv, zl = mesher.fiber_mesh(sim.verts["pos"], sim.qs, sim.verts["lRest"], sim.verts["flags"],
+                                       m.radius, m.barrierThickness)
+    assert list(got) == ["fiber", "fuzz"]
+    gv, gl = got["fiber"]
+    assert gv.shape == fv.shape and gl == fl
+    assert len(fl) == 16  # 8 fibres x 2 yarns
+    np.testing.assert_allclose(gv, fv, rtol=0, atol=2e-6)
+    hv, hl = got["fuzz"]
+    assert hv.shape == zv.shape and [tuple(x) for x in hl] == zl and len(zl) > 100
+    np.testing.assert_allclose(hv, zv, rtol=0, atol=2e-6)
+    with pytest.raises(RuntimeError):
+        sim.exportFiberMesh("/nonexistent-dir/f.obj")
+    sim.close()

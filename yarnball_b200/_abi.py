@@ -118,6 +118,7 @@ SIGNATURES = {
     "yb_scene_range": (ctypes.c_int, [_P, ctypes.c_int32, c_int32_p, c_int32_p]),
     "yb_export_bcc": (ctypes.c_int, [_P, ctypes.c_char_p, ctypes.c_int32]),
     "yb_export_obj": (ctypes.c_int, [_P, ctypes.c_char_p]),
+    "yb_export_fiber_mesh": (ctypes.c_int, [_P, ctypes.c_char_p]),
     "yb_save_state": (ctypes.c_int, [_P, ctypes.c_char_p]),
     "yb_read_bcc": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_float, c_float_p, ctypes.c_int32, ctypes.c_int32,
                                    ctypes.POINTER(_P)]),

@@ -571,6 +571,10 @@ bool ends_with(const std::string& s, const char* suf) {
 
 }  // namespace
 
+namespace yb {
+void set_io_error(const std::string& msg) { g_ioError = msg; }
+}  // namespace yb
+
 // =========================================================================================
 extern "C" {
 

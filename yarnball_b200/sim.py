@@ -265,6 +265,10 @@ class Sim:
         """Sim::exportToOBJ (io/fileExport.cpp:65-100)."""
         check(self._lib.yb_export_obj(self._h, os.fsencode(path)), "exportToOBJ")
 
+    def exportFiberMesh(self, path):
+        """Sim::exportFiberMesh (io/fiberMesher.cpp:9-157): fibres and fuzz as OBJ polylines."""
+        check(self._lib.yb_export_fiber_mesh(self._h, os.fsencode(path)), "exportFiberMesh")
+
     def save_state(self, path):
         """Full-state checkpoint; Sim.load_state(path) continues bit-identically."""
         check(self._lib.yb_save_state(self._h, os.fsencode(path)), "save_state")
