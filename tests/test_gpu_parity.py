@@ -214,3 +214,22 @@ def test_device_pin_driver_follows_prescribed_rotation():
     assert np.abs(pa[top] - expect).max() < 2e-6
     a.close()
     b.close()
+
+
+def test_upload_rejects_bad_connection_index_and_keeps_the_state():
+    """upload() validates connection indices on host threads while the copies run; a bad
+    index is rejected before the device state changes, and the simulation stays usable."""
+    sim = scenes.build_readme()
+    sim.advance(1 / 30.0)
+    sim.download()
+    before = sim.read_state_f64()[0]
+    good = sim.verts["connectionIndex"].copy()
+    sim.verts["connectionIndex"][5] = sim.numVerts + 7
+    with pytest.raises(RuntimeError):
+        sim.upload()
+    np.testing.assert_array_equal(sim.read_state_f64()[0], before)
+    sim.verts["connectionIndex"][:] = good
+    sim.upload()
+    sim.advance(1 / 30.0)
+    assert np.all(np.isfinite(sim.read_state_f64()[0]))
+    sim.close()

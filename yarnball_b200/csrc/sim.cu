@@ -16,12 +16,14 @@
 // advection.  No step reads anything back to the host (the reference's BVH query returns
 // its pair count to the host every detection); each of the three substep shapes is captured
 // once as a CUDA graph and replayed.
+#include <algorithm>
 #include <cmath>
 #include <cfloat>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <new>
+#include <thread>
 #include <vector>
 
 #include "yarnball_b200.h"
@@ -570,38 +572,88 @@ struct Engine : EngineBase {
     yb_status upload() override {
         const size_t n = (size_t)S->n;
         const size_t cap = (size_t)S->capVerts;
-        // Segment list and connection validation from the host flags.
-        std::vector<int> segs;
-        segs.reserve(n);
-        for (int s = 0; s < S->numScenes; s++) {
-            for (int i = S->sceneOff[s]; i < S->sceneOff[s + 1]; i++) {
-                const int c = S->verts[i].connectionIndex;
-                if (c >= S->n || c < -1) return YB_ERR_INVALID_ARGUMENT;
-                if (i + 1 < S->sceneOff[s + 1] && has(S->verts[i].flags, YB_HAS_NEXT)) segs.push_back(i);
-            }
-        }
         char* sv = stage;
         char* svel = sv + sizeof(yb_vertex) * cap;
         char* sq = svel + 12 * cap;
         char* sqr = sq + 16 * cap;
         cudaStream_t st = S->stream;
+        // The copies into the staging buffers run while the host validates connections and
+        // rebuilds the segment list; the device state changes only in convert_in, launched
+        // after the host pass has accepted the input.
         YB_CUDA(cudaMemcpyAsync(sv, S->verts, sizeof(yb_vertex) * n, cudaMemcpyHostToDevice, st));
         YB_CUDA(cudaMemcpyAsync(svel, S->vels, 12 * n, cudaMemcpyHostToDevice, st));
         YB_CUDA(cudaMemcpyAsync(sq, S->qs, 16 * n, cudaMemcpyHostToDevice, st));
         YB_CUDA(cudaMemcpyAsync(sqr, S->qRests, 16 * n, cudaMemcpyHostToDevice, st));
-        if (!segs.empty())
-            YB_CUDA(cudaMemcpyAsync(d.segs, segs.data(), sizeof(int) * segs.size(), cudaMemcpyHostToDevice, st));
+        bool changed = false;
+        const bool ok = host_segments(changed);
+        if (!ok) {
+            cudaStreamSynchronize(st);
+            return YB_ERR_INVALID_ARGUMENT;
+        }
+        if (changed && !S->segs.empty())
+            YB_CUDA(cudaMemcpyAsync(d.segs, S->segs.data(), sizeof(int) * S->segs.size(), cudaMemcpyHostToDevice, st));
         launch_convert_in(d, sv, (const float*)svel, (const float*)sq, (const float*)sqr, sceneOf, st);
         S->launches++;
         YB_CUDA(cudaGetLastError());
         YB_CUDA(cudaStreamSynchronize(st));
-        if ((int)segs.size() != d.nseg || segs != S->segs) {
-            d.nseg = (int)segs.size();
-            S->segs.swap(segs);
+        if (changed) {
+            d.nseg = (int)S->segs.size();
             S->lastBVHRebuild = INFINITY;  // topology must be rebuilt
             invalidate_graphs();
         }
         return YB_OK;
+    }
+
+    // Segment list (vertices with hasNext that are not the last of their scene) and
+    // connection-index validation from the host arrays, on host threads.  Replaces S->segs and
+    // sets `changed` when the list differs from the previous one; false on an invalid index.
+    bool host_segments(bool& changed) {
+        const int n = S->n;
+        const int T = std::max(1, std::min<int>(16, std::min<int>((int)std::thread::hardware_concurrency(),
+                                                                   (n + 262143) / 262144)));
+        std::vector<int> cnt(T, 0);
+        std::vector<char> bad(T, 0);
+        auto seg_here = [&](int i, int sceneEnd) { return i + 1 < sceneEnd && has(S->verts[i].flags, YB_HAS_NEXT); };
+        auto scene_end = [&](int i) {  // end of the scene holding vertex i
+            return *std::upper_bound(S->sceneOff.begin(), S->sceneOff.end(), i);
+        };
+        auto run = [&](auto&& body) {
+            std::vector<std::thread> th;
+            for (int t = 1; t < T; t++) th.emplace_back(body, t);
+            body(0);
+            for (auto& x : th) x.join();
+        };
+        run([&](int t) {
+            const int a = (int)((long long)n * t / T), b = (int)((long long)n * (t + 1) / T);
+            int c = 0, end = a < n ? scene_end(a) : n;
+            for (int i = a; i < b; i++) {
+                if (i >= end) end = scene_end(i);
+                const int ci = S->verts[i].connectionIndex;
+                if (ci >= n || ci < -1) bad[t] = 1;
+                c += seg_here(i, end);
+            }
+            cnt[t] = c;
+        });
+        for (int t = 0; t < T; t++)
+            if (bad[t]) return false;
+        std::vector<int> off(T + 1, 0);
+        for (int t = 0; t < T; t++) off[t + 1] = off[t] + cnt[t];
+        std::vector<int> segs(off[T]);
+        const bool sameSize = S->segs.size() == segs.size();
+        std::vector<char> diff(T, 0);
+        run([&](int t) {
+            const int a = (int)((long long)n * t / T), b = (int)((long long)n * (t + 1) / T);
+            int k = off[t], end = a < n ? scene_end(a) : n;
+            for (int i = a; i < b; i++) {
+                if (i >= end) end = scene_end(i);
+                if (seg_here(i, end)) segs[k++] = i;
+            }
+            if (sameSize) diff[t] = !std::equal(segs.begin() + off[t], segs.begin() + off[t + 1], S->segs.begin() + off[t]);
+        });
+        changed = !sameSize;
+        for (int t = 0; t < T; t++) changed = changed || diff[t];
+        if (changed) S->segs.swap(segs);
+        return true;
     }
 
     yb_status download() override {
