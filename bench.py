@@ -340,6 +340,9 @@ def run_ours(args):
     cpu = None
     if not args.no_cpu and rank == 0 and world == 1:
         cpu = cpu_baseline_sample(spec)
+    acc = None
+    if rank == 0:
+        acc = accuracy_sample(spec, (tune_threads, tune_lanes, tune_pipe))
 
     if rank == 0:
         out = {
@@ -351,12 +354,38 @@ def run_ours(args):
             "batched_over_plain": (value / plain["value"]) if plain else None,
             "contacts": {"pairs": total_pairs, "segments_with_contacts": segs_with, "max_per_segment": max_cols,
                          "cbar": cbar},
-            "interpenetrations": pens, "diagnostics": diag,
+            "interpenetrations": pens, "diagnostics": diag, "accuracy": acc,
         }
         print(json.dumps(out))
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def accuracy_sample(spec, shape, target_verts=1_000_000):
+    """FP32 production build against the FP64 build of the same kernels (which the tests tie to
+    the FP64 CPU oracle) on the first scenes of the workload (about 1M vertices), one frame from
+    the same state: max position difference over max displacement."""
+    from yarnball_b200 import scenes, sharding
+
+    yarns, lens, kbend = spec
+    k, tot = 0, 0
+    while k < len(lens) and tot < target_verts:
+        tot += int(lens[k].sum())
+        k += 1
+    sub = sharding.subset_spec(spec, list(range(k)))
+    out = {}
+    for prec in ("fp32", "fp64"):
+        sim, _ = scenes.build_batched(seed=SEED, spec=sub, precision=prec)
+        sim.set_tuning(shape[0], shape[1], True, bool(shape[2]))
+        x0 = sim.read_state_f64()[0]
+        sim.advance(FRAME)
+        out[prec] = sim.read_state_f64()[0]
+        sim.close()
+    disp = float(np.abs(out["fp64"] - x0).max())
+    err = float(np.abs(out["fp32"] - out["fp64"]).max())
+    return {"vs": "FP64 build of the same kernels", "rel_err_1_frame": err / disp, "max_abs_err_m": err,
+            "max_displacement_m": disp, "vertices": tot, "scenes": k, "frames": 1, "bound": 1e-4}
 
 
 def run_plain(spec, stream, shape):
