@@ -346,6 +346,11 @@ struct Engine : EngineBase {
         want((void**)&d.nodes, sizeof(BNode<R>) * nn);
         want((void**)&d.wide, sizeof(WNode<R>) * nn);
         want((void**)&d.qrec, sizeof(QRec<R>) * n);
+        want((void**)&d.brec, sizeof(QRec<R>) * n);
+        want((void**)&d.nbkt, sizeof(int) * 4);
+        want((void**)&d.sceneFirst, sizeof(int) * ns);
+        want((void**)&d.sceneLastSeg, sizeof(int) * ns);
+        want((void**)&d.sceneBkt, sizeof(int) * ns);
         want((void**)&d.nodeLast, sizeof(int) * nn);
         want((void**)&d.leafParent, sizeof(int) * n);
         want((void**)&d.refitCount, sizeof(unsigned) * nn);
@@ -699,10 +704,10 @@ struct Engine : EngineBase {
             if (rebuild) {
                 launch_bvh_rebuild(d, st, sortScratch, sortBytes, keyBits);
                 const int passes = d.nseg > 1 ? (keyBits + 7) / 8 : 0;
-                k += 3 + (d.nseg > 1 ? 2 + passes : 0) + 1 + 1;
+                k += 3 + (d.nseg > 1 ? 2 + passes : 0) + 3 + 1 + 2;
             } else {
                 launch_bvh_refit(d, st);
-                k += 1;
+                k += 2;
             }
             launch_traverse(d, st); k += 2;
         } else {
@@ -872,11 +877,11 @@ struct Engine : EngineBase {
                 mark(1);
                 launch_bvh_rebuild(d, st, sortScratch, sortBytes, keyBits);
                 const int passes = d.nseg > 1 ? (keyBits + 7) / 8 : 0;
-                launches[1] += 3 + (d.nseg > 1 ? 2 + passes : 0) + 1 + 1;
+                launches[1] += 3 + (d.nseg > 1 ? 2 + passes : 0) + 3 + 1 + 2;
             } else {
                 mark(2);
                 launch_bvh_refit(d, st);
-                launches[2] += 1;
+                launches[2] += 2;
             }
             mark(3);
             launch_traverse(d, st); launches[3] += 2;
