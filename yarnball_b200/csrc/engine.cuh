@@ -117,9 +117,6 @@ struct alignas(16) WNode {
 
 // Query record of a sorted leaf, written by the refit for the traversal: the segment's padded
 // box, the segment and its scene (one coalesced load when a lane starts a query).
-// BVH leaves are buckets of up to BKT consecutive sorted segments of one scene.
-constexpr int BKT = 4;
-
 template <typename R>
 struct alignas(16) QRec {
     R mn[3], mx[3];
@@ -150,12 +147,7 @@ struct Dev {
     // BVH
     BNode<R>* nodes;  // nseg - 1 internal nodes
     WNode<R>* wide;   // nseg - 1 wide nodes (rebuilt after every refit)
-    QRec<R>* qrec;    // per sorted segment: box, segment, scene (written by the refit)
-    QRec<R>* brec;    // per leaf bucket: union box, (first sorted position << 3) | members, scene
-    int* nbkt;        // number of leaf buckets (device value, written at every rebuild)
-    int* sceneFirst;  // per scene: first and last sorted position of its segments (-1 / -2: none)
-    int* sceneLastSeg;
-    int* sceneBkt;    // per scene: index of its first leaf bucket
+    QRec<R>* qrec;    // per sorted leaf: box, segment, scene (written by the refit)
     int* nodeLast;    // sorted position of the last leaf of each internal node's range
     int* leafParent;  // per sorted leaf position
     unsigned* refitCount;

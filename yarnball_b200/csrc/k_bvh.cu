@@ -6,15 +6,13 @@
 //   * leaf keys: 30-bit Morton code of the segment midpoint, normalised by its scene's
 //     bounds, with the scene id above bit 30 so that every scene is one subtree;
 //   * stable LSD radix sort of (key, segment) pairs (k_sort.cu);
-//   * leaves are buckets of up to 4 consecutive sorted segments of one scene;
-//   * Karras 2012 binary radix tree emission over the buckets, one thread per internal node,
-//     ties between equal keys broken by leaf position;
-//   * bottom-up AABB refit with one atomic arrival counter per internal node, then a 4-wide
-//     view of the tree for the traversal;
-//   * traversal: every bucket walks its own scene's subtree with the union box of its members;
-//     member pairs whose padded boxes overlap go through the narrow-phase filter (detect.cuh)
-//     and kept pairs are appended to both segments' lists, which are then sorted by partner id
-//     before the step-size limit is computed from them.
+//   * Karras 2012 binary radix tree emission, one thread per internal node, ties between
+//     equal keys broken by leaf position;
+//   * bottom-up AABB refit with one atomic arrival counter per internal node;
+//   * traversal: every segment walks its own scene's subtree with its own padded box and
+//     keeps the partners that pass the narrow-phase filter (detect.cuh).  Each segment
+//     writes only its own list (no atomics on other segments' lists); the list is then
+//     sorted by partner id and the step-size limit is computed from it in the same thread.
 #include "detect.cuh"
 
 namespace yb {
@@ -37,8 +35,6 @@ __global__ void k_scene_box_init(Dev<R> d) {
         d.sceneBox[6 * s + 3 + a] = 0u;
     }
     d.sceneRoot[s] = INT_MIN;
-    d.sceneFirst[s] = -1;
-    d.sceneLastSeg[s] = -2;
 }
 
 // Per-scene bounds of segment midpoints (Morton normalisation).
@@ -105,77 +101,19 @@ __device__ __forceinline__ int kdelta(const unsigned long long* __restrict__ key
     return __clzll(a ^ b);
 }
 
-// Leaf buckets: runs of up to BKT consecutive sorted segments inside one scene (sorted keys
-// carry the scene id above bit 30, so a scene's segments are contiguous).  Three steps after
-// the sort: each scene's first and last sorted position, an exclusive scan of its bucket count
-// (one block), then one record per bucket: its key (the first member's) in keys[1] and
-// (first sorted position << 3) | members in vals[1].
+// Karras 2012 internal-node emission + scene subtree roots.
 template <typename R>
-__global__ void __launch_bounds__(256) k_bkt_scene(Dev<R> d) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= d.nseg) return;
-    const unsigned long long* keys = d.keys[0];
-    const int sc = (int)(keys[p] >> 30);
-    if (p == 0 || (int)(keys[p - 1] >> 30) != sc) d.sceneFirst[sc] = p;
-    if (p == d.nseg - 1 || (int)(keys[p + 1] >> 30) != sc) d.sceneLastSeg[sc] = p;
-}
-
-template <typename R>
-__global__ void __launch_bounds__(1024) k_bkt_scan(Dev<R> d) {
-    __shared__ int sWarp[32];
-    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-    int carry = 0;
-    for (int base = 0; base < d.numScenes; base += 1024) {
-        const int s = base + t;
-        int c = 0;
-        if (s < d.numScenes && d.sceneFirst[s] >= 0) c = (d.sceneLastSeg[s] - d.sceneFirst[s] + BKT) / BKT;
-        int x = c;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-        }
-        if (lane == 31) sWarp[w] = x;
-        __syncthreads();
-        int wo = 0, tot = 0;
-        for (int i = 0; i < 32; i++) {
-            if (i < w) wo += sWarp[i];
-            tot += sWarp[i];
-        }
-        if (s < d.numScenes) d.sceneBkt[s] = carry + wo + x - c;
-        carry += tot;
-        __syncthreads();
-    }
-    if (t == 0) *d.nbkt = carry;
-}
-
-template <typename R>
-__global__ void __launch_bounds__(256) k_bkt_form(Dev<R> d) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= d.nseg) return;
-    const unsigned long long key = d.keys[0][p];
-    const int sc = (int)(key >> 30);
-    const int j = p - d.sceneFirst[sc];
-    if (j % BKT) return;
-    const int b = d.sceneBkt[sc] + j / BKT;
-    const int cnt = min(BKT, d.sceneLastSeg[sc] - p + 1);
-    d.keys[1][b] = key;
-    d.vals[1][b] = (p << 3) | cnt;
-}
-
-// Karras 2012 internal-node emission over the leaf buckets (keys[1]) + scene subtree roots.
-// Leaf codes are -(bucket + 1); ranges, splits and scene ends are bucket positions.
-template <typename R>
-__global__ void __launch_bounds__(256) k_karras(Dev<R> d, const unsigned long long* __restrict__ keys) {
-    const int n = *d.nbkt;
+__global__ void __launch_bounds__(256) k_karras(Dev<R> d, const unsigned long long* __restrict__ keys,
+                                                const int* __restrict__ vals) {
+    const int n = d.nseg;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    // scenes of a single bucket
+    // single-leaf scenes
     {
         const unsigned long long sc = keys[i] >> 30;
         const bool lo = (i == 0) || ((keys[i - 1] >> 30) != sc);
         const bool hi = (i == n - 1) || ((keys[i + 1] >> 30) != sc);
-        if (lo && hi) d.sceneRoot[sc] = -(i + 1);
+        if (lo && hi) d.sceneRoot[sc] = -(vals[i] + 1);
     }
     if (i >= n - 1) return;
     const int dir = (kdelta(keys, n, i, i + 1) - kdelta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
@@ -199,14 +137,14 @@ __global__ void __launch_bounds__(256) k_karras(Dev<R> d, const unsigned long lo
     nd.split = gamma;
     d.nodeLast[i] = last;
     if (first == gamma) {
-        nd.left = -(gamma + 1);
+        nd.left = -(vals[gamma] + 1);
         d.leafParent[gamma] = i;
     } else {
         nd.left = gamma;
         d.nodes[gamma].parent = i;
     }
     if (last == gamma + 1) {
-        nd.right = -(gamma + 1 + 1);
+        nd.right = -(vals[gamma + 1] + 1);
         d.leafParent[gamma + 1] = i;
     } else {
         nd.right = gamma + 1;
@@ -232,41 +170,16 @@ __device__ __forceinline__ void store_child_box(BNode<R>& nd, bool left, const B
     }
 }
 
-// Bottom-up refit over the leaf buckets: each bucket's members get their padded boxes from the
-// current positions / velocity radius (written as query records, qrec, at their sorted
-// positions), the bucket's union box (brec) is the leaf box, and unions go upward with one
-// atomic arrival counter per node.  refitCount must be zero on entry (cleared by the launcher).
+// Bottom-up refit: leaf boxes from the current positions/velocity radius, unions upward.
+// refitCount must be zero on entry (cleared by the launcher).
 template <typename R>
-__global__ void __launch_bounds__(256) k_refit(Dev<R> d) {
-    const int bk = blockIdx.x * blockDim.x + threadIdx.x;
-    const int nb = *d.nbkt;
-    if (bk >= nb) return;
-    const int info = d.vals[1][bk];
-    const int start = info >> 3, cnt = info & 7;
-    Box<R> b;
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-        b.mn[a] = yinf<R>();
-        b.mx[a] = -yinf<R>();
-    }
-    int sc = 0;
-    for (int m = 0; m < cnt; m++) {
-        const int p = start + m;
-        const int k = d.vals[0][p];
-        sc = scene_of(d.vp[k].flags);
-        const Box<R> sb = segment_box(d, k, d.sp[sc]);
-        QRec<R> r;
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-            r.mn[a] = sb.mn[a];
-            r.mx[a] = sb.mx[a];
-            b.mn[a] = ymin(b.mn[a], sb.mn[a]);
-            b.mx[a] = ymax(b.mx[a], sb.mx[a]);
-        }
-        r.k = k;
-        r.sc = sc;
-        d.qrec[p] = r;
-    }
+__global__ void __launch_bounds__(256) k_refit(Dev<R> d, const int* __restrict__ sortedVals) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= d.nseg) return;
+    const int k = sortedVals[p];
+    const int sc = scene_of(d.vp[k].flags);
+    const SceneParams<R>& sp = d.sp[sc];
+    Box<R> b = segment_box(d, k, sp);
     {
         QRec<R> r;
 #pragma unroll
@@ -274,16 +187,16 @@ __global__ void __launch_bounds__(256) k_refit(Dev<R> d) {
             r.mn[a] = b.mn[a];
             r.mx[a] = b.mx[a];
         }
-        r.k = info;
+        r.k = k;
         r.sc = sc;
-        d.brec[bk] = r;
+        d.qrec[p] = r;
     }
-    if (nb == 1) return;
-    int code = -(bk + 1);
-    int node = d.leafParent[bk];
+    int code = -(k + 1);
+    if (d.nseg == 1) return;
+    int node = d.leafParent[p];
     int guard = 0;
     while (node >= 0) {
-        if (node >= nb - 1) {  // only a corrupt tree gets here: report, touch nothing
+        if (node >= d.nseg - 1) {  // only a corrupt tree gets here: report, touch nothing
             atomicOr(&d.err[EW_INTERNAL], IE_REFIT);
             return;
         }
@@ -317,7 +230,7 @@ __global__ void __launch_bounds__(256) k_refit(Dev<R> d) {
 template <typename R>
 __global__ void __launch_bounds__(256) k_widen(Dev<R> d) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= *d.nbkt - 1) return;
+    if (i >= d.nseg - 1) return;
     const BNode<R> nd = d.nodes[i];
     WNode<R> w;
     int e = 0;
@@ -355,7 +268,7 @@ __global__ void __launch_bounds__(256) k_widen(Dev<R> d) {
 constexpr int BVH_STACK = 96;
 constexpr int TRAV_THREADS = 128;
 constexpr int TRAV_WARPS = TRAV_THREADS / 32;
-constexpr int TRAV_QCAP = 192;      // < 32 left over + up to 5 bucket pairs per lane (own + 4 leaves)
+constexpr int TRAV_QCAP = 160;      // < 32 left over + up to 4 candidates per lane
 
 // Appends y to x's contact list.  The count keeps growing past MAX_COLS so that the list
 // kernel can report the overflow (collision.cu:80-90).
@@ -365,21 +278,19 @@ __device__ __forceinline__ void list_append(const Dev<R>& d, int x, int y) {
     if (pos < MAX_COLS) d.cols[col_at(x, pos)] = y;
 }
 
-// Broadphase + narrow phase.  Every leaf bucket queries the tree once with the union box of
-// its members (buckets are taken in sorted order, so neighbouring lanes start on neighbouring
-// queries).  Each pair of buckets is found by exactly one of them: the one with the lower
-// position, whose walk skips every entry holding only buckets at or before its own; pairs
-// inside a bucket are handled when its query starts.  The walk runs over the wide nodes (four
-// grandchildren per node), with a per-lane stack; a lane that finishes takes the next
-// unprocessed bucket from a global counter (one atomic per warp and refill), so a warp keeps
-// its 32 lanes busy until the buckets run out (persistent grid).
-// Two per-warp queues: a bucket pair (own, other) whose union boxes overlap goes into the
-// first; whenever 32 are queued each lane expands one, testing the members' own padded boxes
-// against each other, and member pairs that overlap go into the second queue; whenever 32 of
-// those are queued the warp runs the separately rounded narrow-phase test on them, one pair
-// per lane, with the lower segment index as segment A, and appends kept pairs to both lists.
-// The pair set is the same as an all-pairs test: every pair of overlapping member boxes lies
-// in overlapping bucket boxes, each bucket pair is expanded once, and the test is symmetric.
+// Broadphase + narrow phase.  Every segment queries the tree once with its own box (the
+// sorted leaves of the last rebuild, taken in Morton order, so neighbouring lanes start on
+// neighbouring queries).  Each unordered pair is found by exactly one of its two segments:
+// the one with the lower sorted position, whose walk skips every entry holding only leaves at
+// or before its own position.  The walk runs over the wide nodes (four grandchildren per
+// node), so a query takes half as many dependent node loads as on the binary tree.  Lanes walk
+// independently, with a per-lane stack; a lane that finishes takes the next unprocessed query
+// from a global counter (one atomic per warp and refill), so a warp keeps all 32 lanes busy
+// until the queries run out (persistent grid).  A leaf entry that overlaps a lane's box
+// becomes a candidate pair in a per-warp queue; whenever 32 candidates are queued the warp
+// runs the separately rounded narrow-phase test on them, one pair per lane, with the lower
+// segment index as segment A, and appends kept pairs to both lists.  The pair set is the same
+// as an all-pairs test: the test is symmetric and every overlapping pair is visited once.
 template <typename R>
 __device__ __forceinline__ void trav_load_wide(const WNode<R>* wide, int node, WNode<R>& w) {
     if constexpr (sizeof(R) == 4) {  // one wide node = eight 16-byte loads
@@ -393,88 +304,58 @@ __device__ __forceinline__ void trav_load_wide(const WNode<R>* wide, int node, W
 }
 
 template <typename R>
-__device__ __forceinline__ void load_rec(const QRec<R>* recs, int i, QRec<R>& r) {
-    if constexpr (sizeof(R) == 4) {
-        const float4* src = reinterpret_cast<const float4*>(recs + i);
-        float4* dst = reinterpret_cast<float4*>(&r);
-        dst[0] = __ldg(src);
-        dst[1] = __ldg(src + 1);
-    } else {
-        r = recs[i];
-    }
-}
-
-template <typename R>
-__device__ __forceinline__ bool rec_overlap(const QRec<R>& a, const QRec<R>& b) {
-    return a.mn[0] <= b.mx[0] && b.mn[0] <= a.mx[0] && a.mn[1] <= b.mx[1] && b.mn[1] <= a.mx[1] &&
-           a.mn[2] <= b.mx[2] && b.mn[2] <= a.mx[2];
-}
-
-constexpr int TRAV_Q2CAP = 64;  // < 32 left over + at most one member pair per lane per step
-
-template <typename R>
 __global__ void __launch_bounds__(TRAV_THREADS) k_traverse(Dev<R> d) {
-    __shared__ int sB1[TRAV_WARPS][TRAV_QCAP];   // bucket pairs (own, other); other == own: inside
-    __shared__ int sC1[TRAV_WARPS][TRAV_QCAP];
-    __shared__ int sX2[TRAV_WARPS][TRAV_Q2CAP];  // member (segment) pairs, lower index first
-    __shared__ int sY2[TRAV_WARPS][TRAV_Q2CAP];
+    __shared__ int sQx[TRAV_WARPS][TRAV_QCAP];
+    __shared__ int sQy[TRAV_WARPS][TRAV_QCAP];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
-    const int nb = *d.nbkt;
+    const int nseg = d.nseg;
     int stack[BVH_STACK];
     int top = 0;
-    int qi = 0, node = -1;  // query: bucket position, walk state
-    int steps = 0;          // wide nodes visited by this query (a valid walk visits fewer than nb)
+    int qi = 0, k = -1, node = -1;  // query: sorted position, segment, walk state
+    int steps = 0;                  // wide nodes visited by this query (a valid walk visits fewer than nseg)
     bool walking = false;
     Box<R> qb;
-    int q1 = 0, q2 = 0;    // queued entries (identical in every lane)
-    bool more = true;      // the counter has not run out (warp-uniform)
-
-    // Runs the narrow phase on the last m queued member pairs (m <= 32).
-    auto flush2 = [&](int m) {
-        if (lane < m) {
-            const int x = sX2[warp][q2 - m + lane];
-            const int y = sY2[warp][q2 - m + lane];
-            if (pair_keep(d, x, y, d.sp[scene_of(d.vp[x].flags)])) {
-                list_append(d, x, y);
-                list_append(d, y, x);
-            }
-        }
-        q2 -= m;
-        __syncwarp();
-    };
-
+    int qn = 0;        // queued candidates (identical in every lane)
+    bool more = true;  // the counter has not run out (warp-uniform)
     while (true) {
+        // Refill lanes without a walk.
         const unsigned idle = __ballot_sync(0xffffffffu, !walking);
-        bool self = false;  // this lane starts a bucket with at least two members
         if (more && idle) {
             int base = 0;
             if (lane == 0) base = (int)atomicAdd(d.travNext, (unsigned)__popc(idle));
             base = __shfl_sync(0xffffffffu, base, 0);
-            if (base + __popc(idle) >= nb) more = false;
+            if (base + __popc(idle) >= nseg) more = false;
             if (!walking) {
                 qi = base + __popc(idle & lt);
-                if (qi < nb) {
+                if (qi < nseg) {
                     QRec<R> r;
-                    load_rec(d.brec, qi, r);
+                    if constexpr (sizeof(R) == 4) {
+                        const float4* src = reinterpret_cast<const float4*>(d.qrec + qi);
+                        float4* dst = reinterpret_cast<float4*>(&r);
+                        dst[0] = __ldg(src);
+                        dst[1] = __ldg(src + 1);
+                    } else {
+                        r = d.qrec[qi];
+                    }
+                    k = r.k;
+                    const int sc = r.sc;
 #pragma unroll
                     for (int a = 0; a < 3; a++) {
                         qb.mn[a] = r.mn[a];
                         qb.mx[a] = r.mx[a];
                     }
-                    self = (r.k & 7) >= 2;
-                    node = d.sceneRoot[r.sc];
+                    node = d.sceneRoot[sc];
                     top = 0;
                     steps = 0;
-                    walking = node >= 0 && d.sceneLast[r.sc] > qi;  // a leaf root has no other bucket
+                    walking = node >= 0 && d.sceneLast[sc] > qi;  // a leaf root has no pairs
                 }
             }
         }
-        if (!more && !__any_sync(0xffffffffu, walking) && q1 == 0 && q2 == 0) break;
-        int cand[5];
+        if (!more && !__any_sync(0xffffffffu, walking) && qn == 0) break;
+        int cand[4];
         int nc = 0;
-        if (self) cand[nc++] = qi;
-        if (walking && (node >= nb - 1 || ++steps > nb)) {  // only a corrupt tree gets here
+        if (walking && (node >= nseg - 1 || ++steps > nseg)) {  // only a corrupt tree gets here
             atomicOr(&d.err[EW_INTERNAL], IE_BVH_STACK);
             walking = false;
         }
@@ -507,73 +388,37 @@ __global__ void __launch_bounds__(TRAV_THREADS) k_traverse(Dev<R> d) {
                 walking = false;
             }
         }
-        // queue this lane's bucket pairs at its offset (warp scan of the counts)
+        // queue this lane's candidates at its offset (warp scan of the counts)
         int incl = nc;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const int y = __shfl_up_sync(0xffffffffu, incl, o);
             if (lane >= o) incl += y;
         }
-        const int at = q1 + incl - nc;
+        const int at = qn + incl - nc;
 #pragma unroll
-        for (int e = 0; e < 5; e++) {
+        for (int e = 0; e < 4; e++) {
             if (e < nc) {
-                sB1[warp][at + e] = qi;
-                sC1[warp][at + e] = cand[e];
+                sQx[warp][at + e] = min(k, cand[e]);
+                sQy[warp][at + e] = max(k, cand[e]);
             }
         }
-        q1 += __shfl_sync(0xffffffffu, incl, 31);
+        qn += __shfl_sync(0xffffffffu, incl, 31);
         __syncwarp();
         const bool drain = !more && !__any_sync(0xffffffffu, walking);
-        while (q1 >= 32 || (drain && q1 > 0)) {
-            // each lane expands one bucket pair into member pairs whose boxes overlap
-            const int m = min(q1, 32);
-            int sb = 0, nbm = 0, scn = 0, ncm = 0;
-            bool inside = false;
+        while (qn >= 32 || (drain && qn > 0)) {
+            const int m = min(qn, 32);
             if (lane < m) {
-                const int b = sB1[warp][q1 - m + lane];
-                const int c = sC1[warp][q1 - m + lane];
-                QRec<R> rb, rc;
-                load_rec(d.brec, b, rb);
-                load_rec(d.brec, c, rc);
-                sb = rb.k >> 3;
-                nbm = rb.k & 7;
-                scn = rc.k >> 3;
-                ncm = rc.k & 7;
-                inside = b == c;
-            }
-            q1 -= m;
-            __syncwarp();
-            for (int i = 0; i < BKT; i++) {
-                QRec<R> ri;
-                const bool vi = i < nbm;
-                if (vi) load_rec(d.qrec, sb + i, ri);
-                for (int jj = 0; jj < BKT; jj++) {
-                    bool hit = false;
-                    int x = 0, y = 0;
-                    if (vi && jj < ncm && (!inside || i < jj)) {
-                        QRec<R> rj;
-                        load_rec(d.qrec, scn + jj, rj);
-                        if (rec_overlap(ri, rj)) {
-                            hit = true;
-                            x = min(ri.k, rj.k);
-                            y = max(ri.k, rj.k);
-                        }
-                    }
-                    const unsigned bh = __ballot_sync(0xffffffffu, hit);
-                    if (hit) {
-                        const int a2 = q2 + __popc(bh & lt);
-                        sX2[warp][a2] = x;
-                        sY2[warp][a2] = y;
-                    }
-                    q2 += __popc(bh);
-                    __syncwarp();
-                    if (q2 >= 32) flush2(32);
+                const int x = sQx[warp][qn - m + lane];
+                const int y = sQy[warp][qn - m + lane];
+                if (pair_keep(d, x, y, d.sp[scene_of(d.vp[x].flags)])) {
+                    list_append(d, x, y);
+                    list_append(d, y, x);
                 }
             }
+            qn -= m;
+            __syncwarp();
         }
-        if (drain && q1 == 0)
-            while (q2 > 0) flush2(min(q2, 32));
     }
 }
 
@@ -617,15 +462,12 @@ void launch_bvh_rebuild(const Dev<R>& d, cudaStream_t s, void* sortScratch, size
     unsigned long long* keys[2] = {d.keys[0], d.keys[1]};
     int* vals[2] = {d.vals[0], d.vals[1]};
     const int buf = radix_sort_pairs(keys, vals, d.nseg, keyBits, sortScratch, d.err + EW_INTERNAL, s);
-    // After sorting, buffer 0 must hold the sorted pairs; buffer 1 then holds the buckets.
+    // After sorting, buffer 0 must hold the sorted pairs (refit/karras read it).
     if (buf != 0) {
         cudaMemcpyAsync(d.keys[0], d.keys[1], sizeof(unsigned long long) * d.nseg, cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(d.vals[0], d.vals[1], sizeof(int) * d.nseg, cudaMemcpyDeviceToDevice, s);
     }
-    k_bkt_scene<R><<<nb, 256, 0, s>>>(d);
-    k_bkt_scan<R><<<1, 1024, 0, s>>>(d);
-    k_bkt_form<R><<<nb, 256, 0, s>>>(d);
-    k_karras<R><<<nb, 256, 0, s>>>(d, d.keys[1]);
+    k_karras<R><<<nb, 256, 0, s>>>(d, d.keys[0], d.vals[0]);
     launch_bvh_refit(d, s);
 }
 
@@ -634,14 +476,12 @@ void launch_bvh_reset(const Dev<R>& d, cudaStream_t s) {
     if (d.numScenes > 0) k_scene_box_init<R><<<(d.numScenes + 127) / 128, 128, 0, s>>>(d);
 }
 
-// Grids are sized for nseg leaves; the kernels read the bucket count on the device.
 template <typename R>
 void launch_bvh_refit(const Dev<R>& d, cudaStream_t s) {
-    if (d.nseg <= 0) return;
+    if (d.nseg <= 0) return;  // one segment: no internal node, but its query record is written
     if (d.nseg > 1) cudaMemsetAsync(d.refitCount, 0, sizeof(unsigned) * (d.nseg - 1), s);
-    const int nb = (d.nseg + 255) / 256;
-    k_refit<R><<<nb, 256, 0, s>>>(d);
-    k_widen<R><<<nb, 256, 0, s>>>(d);
+    k_refit<R><<<(d.nseg + 255) / 256, 256, 0, s>>>(d, d.vals[0]);
+    k_widen<R><<<(d.nseg + 255) / 256, 256, 0, s>>>(d);  // at least one block; the kernel bounds itself
 }
 
 template <typename R>

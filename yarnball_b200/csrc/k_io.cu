@@ -148,9 +148,10 @@ __global__ void k_scene_root_box(Dev<R> d, float* out) {
             b[a] = (float)ymin(nd.lmin[a], nd.rmin[a]);
             b[3 + a] = (float)ymax(nd.lmax[a], nd.rmax[a]);
         }
-    } else if (r != INT_MIN) {  // the scene is one leaf bucket: its union box
-        const QRec<R>& br = d.brec[-r - 1];
-        for (int a = 0; a < 3; a++) { b[a] = (float)br.mn[a]; b[3 + a] = (float)br.mx[a]; }
+    } else if (r != INT_MIN) {
+        const int k = -r - 1;
+        const Box<R> bx = segment_box(d, k, d.sp[s]);
+        for (int a = 0; a < 3; a++) { b[a] = (float)bx.mn[a]; b[3 + a] = (float)bx.mx[a]; }
     }
     for (int a = 0; a < 6; a++) out[6 * s + a] = b[a];
 }

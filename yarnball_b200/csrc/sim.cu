@@ -346,11 +346,6 @@ struct Engine : EngineBase {
         want((void**)&d.nodes, sizeof(BNode<R>) * nn);
         want((void**)&d.wide, sizeof(WNode<R>) * nn);
         want((void**)&d.qrec, sizeof(QRec<R>) * n);
-        want((void**)&d.brec, sizeof(QRec<R>) * n);
-        want((void**)&d.nbkt, sizeof(int) * 4);
-        want((void**)&d.sceneFirst, sizeof(int) * ns);
-        want((void**)&d.sceneLastSeg, sizeof(int) * ns);
-        want((void**)&d.sceneBkt, sizeof(int) * ns);
         want((void**)&d.nodeLast, sizeof(int) * nn);
         want((void**)&d.leafParent, sizeof(int) * n);
         want((void**)&d.refitCount, sizeof(unsigned) * nn);
@@ -704,7 +699,7 @@ struct Engine : EngineBase {
             if (rebuild) {
                 launch_bvh_rebuild(d, st, sortScratch, sortBytes, keyBits);
                 const int passes = d.nseg > 1 ? (keyBits + 7) / 8 : 0;
-                k += 3 + (d.nseg > 1 ? 2 + passes : 0) + 3 + 1 + 2;
+                k += 3 + (d.nseg > 1 ? 2 + passes : 0) + 1 + 2;
             } else {
                 launch_bvh_refit(d, st);
                 k += 2;
@@ -877,7 +872,7 @@ struct Engine : EngineBase {
                 mark(1);
                 launch_bvh_rebuild(d, st, sortScratch, sortBytes, keyBits);
                 const int passes = d.nseg > 1 ? (keyBits + 7) / 8 : 0;
-                launches[1] += 3 + (d.nseg > 1 ? 2 + passes : 0) + 3 + 1 + 2;
+                launches[1] += 3 + (d.nseg > 1 ? 2 + passes : 0) + 1 + 2;
             } else {
                 mark(2);
                 launch_bvh_refit(d, st);
