@@ -445,7 +445,7 @@ def run_serve(args):
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     reqs = serve.poisson_requests(args.rate, args.duration, frames=args.frames)
-    server = serve.Server(budget_bytes=args.budget_gb * 1e9, shape=(128, 1), stream=torch.cuda.Stream())
+    server = serve.Server(budget_bytes=args.budget_gb * 1e9, shape=(128, 0), stream=torch.cuda.Stream())
     pending = list(reqs)
     t0 = time.perf_counter()
     while pending or server.busy():
@@ -468,7 +468,7 @@ def run_serve(args):
     # the same requests, each alone, one after the other (FIFO single server)
     service = []
     for r in reqs:
-        sim = serve.build_request_sim(r, (128, 1))
+        sim = serve.build_request_sim(r, (128, 0))
         st = torch.cuda.Stream()
         sim.set_stream(st.cuda_stream)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -9,7 +9,7 @@ from yarnball_b200 import serve
 
 pytestmark = pytest.mark.gpu
 
-SHAPE = (128, 1)
+SHAPE = (128, 0)
 
 
 def _requests():

@@ -76,7 +76,7 @@ def run_alone(req, shape=None):
 
 
 class Server:
-    def __init__(self, budget_bytes=120e9, shape=(128, 1), bytes_per_vertex=None, capacity_headroom=1.25,
+    def __init__(self, budget_bytes=120e9, shape=(128, 0), bytes_per_vertex=None, capacity_headroom=1.25,
                  stream=None):
         self.budget = float(budget_bytes)
         self.shape = shape
