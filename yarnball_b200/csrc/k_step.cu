@@ -413,10 +413,6 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_bal(Dev<R> d, int src) {
     const D2<R>* __restrict__ DX = d.dx[src];
     const V4<R>* __restrict__ QO = d.q[src];
 
-    __shared__ R sFb[3][B];
-    __shared__ R sHb[6][B];
-    __shared__ R sSL[B];
-    __shared__ R sDX[3][B];
     __shared__ R sSeg[12][B];  // p0, e = p1 - p0, dx, dx1 of each slot's segment
     __shared__ R sCon[2][18][B];  // contributions of one chunk of contacts (double buffered)
     __shared__ int sOwn[2][B];     // owning slot of each contact of a chunk (double buffered)
@@ -536,6 +532,13 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_bal(Dev<R> d, int src) {
             }
         }
     }
+
+    // The halo exchange after the loop uses the contribution buffer the last chunk did not
+    // use (buf): every thread finished reading it before the last chunk's barrier.
+    R (*sFb)[B] = sCon[buf];       // rows 0-2
+    R (*sHb)[B] = sCon[buf] + 3;   // rows 3-8
+    R* sSL = sCon[buf][9];
+    R (*sDX)[B] = sCon[buf] + 10;  // rows 10-12
 
     // the vertex's own terms (cosserat.cu:40-81)
     R sl = yinf<R>();
@@ -899,7 +902,7 @@ void launch_iter(const Dev<R>& d, int srcBuf, int threads, int lanes, int pipe, 
             k_iter_wbal<R, 64, 4><<<(d.n + 61) / 62, 64, 0, s>>>(d, srcBuf);
     } else if (lanes == 0) {  // block-balanced contact loop (shared memory bounds the block size)
         if constexpr (sizeof(R) == 4)
-            k_iter_bal<R, 128, 6><<<(d.n + 125) / 126, 128, 0, s>>>(d, srcBuf);
+            k_iter_bal<R, 128, 7><<<(d.n + 125) / 126, 128, 0, s>>>(d, srcBuf);
         else
             k_iter_bal<R, 64, 4><<<(d.n + 61) / 62, 64, 0, s>>>(d, srcBuf);
     } else if (pipe) {
