@@ -71,42 +71,39 @@ __device__ __forceinline__ bool pair_keep(const Dev<R>& d, int x, int y, const S
     return d2 < E::mul(r, r);
 }
 
-// Step-size limit of segment k over its nc listed contacts.  Also counts contacts whose
-// centre-line distance is at or below 2 * radius (interpenetration), each unordered pair once,
-// and stages the partner endpoints relative to p0 for the first RELCAP contacts (read by
-// every Newton iteration of the substep).
+// Step-size limit (collision.cu:121-159), split so that contacts can be spread over threads:
+// step_limit_base is the per-segment start value, contact_step_limit one contact's bound
+// 0.45 x centre-line distance.  A contact also stages the partner's endpoints relative to p0
+// (for c < RELCAP, read by every Newton iteration of the substep) and reports an
+// interpenetration (distance at or below 2 radius, each unordered pair once, o > k).
 template <typename R>
-__device__ __forceinline__ R segment_step_limit(const Dev<R>& d, int k, const SceneParams<R>& sp, int nc) {
+__device__ __forceinline__ R step_limit_base(const Dev<R>& d, int k, const SceneParams<R>& sp) {
     typedef Ex<R> E;
-    const V3<R> a0 = xyz(d.pos[k]);
-    const V3<R> a1 = xsub(xyz(d.pos[k + 1]), a0);
     R m = sp.stepBase;
     if (sp.useVelRadius) m = E::add(m, E::sqrt(xlen2(xyz(d.dx[0][k].a))));
+    return m;
+}
+
+template <typename R>
+__device__ __forceinline__ R contact_step_limit(const Dev<R>& d, int k, int c, int o, const V3<R>& a0,
+                                                const V3<R>& a1, const SceneParams<R>& sp, bool& pen) {
+    typedef Ex<R> E;
+    const V3<R> b0 = xsub(xyz(d.pos[o]), a0);
+    const V3<R> b1 = xsub(xyz(d.pos[o + 1]), a0);
+    if (c < RELCAP) {
+        const size_t at = rel_at(k, c);
+        d.relA[at] = v4(b0, b1.x);
+        R2<R> rb;
+        rb.x = b1.y;
+        rb.y = b1.z;
+        d.relB[at] = rb;
+    }
+    const UVT<R> uv = closest_uv_exact(a1, b0, b1);
+    const V3<R> nrm = xsub(xscale(uv.u, a1), xmix(b0, b1, uv.v));
+    const R l = E::sqrt(xlen2(nrm));
+    pen = o > k && l <= sp.twoR;
     const R safe = E::mul(E::sub(R(1), R(0.1f)), R(0.5f));
-    int pen = 0;
-    for (int c = 0; c < nc; c++) {
-        const int o = d.cols[col_at(k, c)];
-        const V3<R> b0 = xsub(xyz(d.pos[o]), a0);
-        const V3<R> b1 = xsub(xyz(d.pos[o + 1]), a0);
-        if (c < RELCAP) {
-            const size_t at = rel_at(k, c);
-            d.relA[at] = v4(b0, b1.x);
-            R2<R> rb;
-            rb.x = b1.y;
-            rb.y = b1.z;
-            d.relB[at] = rb;
-        }
-        const UVT<R> uv = closest_uv_exact(a1, b0, b1);
-        const V3<R> nrm = xsub(xscale(uv.u, a1), xmix(b0, b1, uv.v));
-        const R l = E::sqrt(xlen2(nrm));
-        m = ymin(m, E::mul(safe, l));
-        if (o > k && l <= sp.twoR) pen++;
-    }
-    if (pen) {
-        atomicAdd(&d.err[EW_PENETRATIONS], pen);
-        d.err[EW_WARNING] = 2;
-    }
-    return sp.useStepLimit ? m : yinf<R>();
+    return E::mul(safe, l);
 }
 
 }  // namespace yb

@@ -425,31 +425,101 @@ __global__ void __launch_bounds__(TRAV_THREADS) k_traverse(Dev<R> d) {
 // Per segment after the broadphase: clamp and check the count, sort the list by partner id
 // (fixed summation order in the Newton iteration), then the step-size limit.  With
 // sortLists = 0 it only recomputes the step limit from the existing lists (substeps without
-// detection, collision.cu:121-172).
+// detection, collision.cu:121-172).  A block of 128 segments flattens their contact lists
+// (block scan) and evaluates 128 contacts at a time, one per thread; each segment then takes
+// the minimum over its contacts in list order (the minimum is exact, so this equals a
+// per-segment loop).
 template <typename R>
 __global__ void __launch_bounds__(128) k_lists(Dev<R> d, int sortLists) {
-    const int si = blockIdx.x * blockDim.x + threadIdx.x;
-    if (si >= d.nseg) return;
-    const int k = d.segs[si];
-    const SceneParams<R>& sp = d.sp[scene_of(d.vp[k].flags)];
-    int nc = d.numCols[k];
-    if (sortLists) {
-        if (nc > MAX_COLS) d.err[EW_ERROR] = 1;
-        if (nc) atomicMax(&d.err[EW_MAX_COLS], nc);
-        nc = min(nc, MAX_COLS);
-        int* __restrict__ cl = d.cols + col_at(k, 0);
-        for (int a = 1; a < nc; a++) {
-            const int v = cl[a];
-            int b = a - 1;
-            while (b >= 0 && cl[b] > v) {
-                cl[b + 1] = cl[b];
-                b--;
+    constexpr int B = 128;
+    __shared__ int sOff[B + 1];
+    __shared__ int sWarp[B / 32];
+    __shared__ int sSeg[B];
+    __shared__ R sA0[3][B], sA1[3][B];
+    __shared__ int sScene[B];
+    __shared__ R sLim[B];
+    const int t = threadIdx.x;
+    const int si = blockIdx.x * B + t;
+    const bool valid = si < d.nseg;
+    int k = -1, nc = 0, sc = 0;
+    V3<R> a0(R(0)), a1(R(0));
+    if (valid) {
+        k = d.segs[si];
+        sc = scene_of(d.vp[k].flags);
+        nc = d.numCols[k];
+        if (sortLists) {
+            if (nc > MAX_COLS) d.err[EW_ERROR] = 1;
+            if (nc) atomicMax(&d.err[EW_MAX_COLS], nc);
+            nc = min(nc, MAX_COLS);
+            int* __restrict__ cl = d.cols + col_at(k, 0);
+            for (int a = 1; a < nc; a++) {
+                const int v = cl[a];
+                int b = a - 1;
+                while (b >= 0 && cl[b] > v) {
+                    cl[b + 1] = cl[b];
+                    b--;
+                }
+                cl[b + 1] = v;
             }
-            cl[b + 1] = v;
+            d.numCols[k] = nc;
         }
-        d.numCols[k] = nc;
+        a0 = xyz(d.pos[k]);
+        a1 = xsub(xyz(d.pos[k + 1]), a0);
     }
-    d.stepLim[k] = segment_step_limit(d, k, sp, nc);
+    sSeg[t] = k;
+    sScene[t] = sc;
+    sA0[0][t] = a0.x; sA0[1][t] = a0.y; sA0[2][t] = a0.z;
+    sA1[0][t] = a1.x; sA1[1][t] = a1.y; sA1[2][t] = a1.z;
+    {
+        const int lane = t & 31, w = t >> 5;
+        int x = nc;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) sWarp[w] = x;
+        __syncthreads();
+        int wo = 0;
+        for (int i = 0; i < w; i++) wo += sWarp[i];
+        sOff[t] = wo + x - nc;
+        if (t == B - 1) sOff[B] = wo + x;
+        __syncthreads();
+    }
+    const int total = sOff[B];
+    const int myOff = sOff[t];
+    R m = R(0);
+    if (valid) m = step_limit_base(d, k, d.sp[sc]);
+    int pens = 0;
+    for (int base = 0; base < total; base += B) {
+        const int f = base + t;
+        R lim = yinf<R>();
+        if (f < total) {
+            int lo = 0, hi = B - 1;  // owner: the last slot whose offset is <= f
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (sOff[mid] <= f) lo = mid; else hi = mid - 1;
+            }
+            const int s = lo, c = f - sOff[s];
+            const int ks = sSeg[s];
+            const int o = d.cols[col_at(ks, c)];
+            const V3<R> oa0(sA0[0][s], sA0[1][s], sA0[2][s]);
+            const V3<R> oa1(sA1[0][s], sA1[1][s], sA1[2][s]);
+            bool pen = false;
+            lim = contact_step_limit(d, ks, c, o, oa0, oa1, d.sp[sScene[s]], pen);
+            pens += pen;
+        }
+        sLim[t] = lim;
+        __syncthreads();
+        const int f0 = max(myOff, base), f1 = min(myOff + nc, base + B);
+        for (int g = f0; g < f1; g++) m = ymin(m, sLim[g - base]);
+        __syncthreads();
+    }
+    if (pens) {
+        atomicAdd(&d.err[EW_PENETRATIONS], pens);
+        d.err[EW_WARNING] = 2;
+    }
+    if (valid) d.stepLim[k] = d.sp[sc].useStepLimit ? m : yinf<R>();
 }
 
 template <typename R>
