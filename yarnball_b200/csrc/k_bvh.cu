@@ -13,6 +13,8 @@
 //     keeps the partners that pass the narrow-phase filter (detect.cuh).  Each segment
 //     writes only its own list (no atomics on other segments' lists); the list is then
 //     sorted by partner id and the step-size limit is computed from it in the same thread.
+#include <cuda/atomic>
+
 #include "detect.cuh"
 
 namespace yb {
@@ -203,10 +205,12 @@ __global__ void __launch_bounds__(256) k_refit(Dev<R> d, const int* __restrict__
         BNode<R>& nd = d.nodes[node];
         const bool isLeft = (nd.left == code);
         store_child_box(nd, isLeft, b);
-        __threadfence();
-        const unsigned old = atomicAdd(&d.refitCount[node], 1u);
+        // device-scope acquire-release: the first arrival's box stores are visible to the
+        // second arrival, which finishes the node
+        const unsigned old =
+            cuda::atomic_ref<unsigned, cuda::thread_scope_device>(d.refitCount[node]).fetch_add(
+                1u, cuda::memory_order_acq_rel);
         if (old == 0u) return;  // first arrival: the sibling finishes this node
-        __threadfence();
         const R* omn = isLeft ? nd.rmin : nd.lmin;
         const R* omx = isLeft ? nd.rmax : nd.lmax;
 #pragma unroll
