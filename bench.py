@@ -16,6 +16,7 @@ collective on the data path; the time is the max over ranks of the device time.
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -51,10 +52,11 @@ def parse():
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     p.add_argument("--cap", type=int, default=8388608, help="vertex cap of the batched workload")
     p.add_argument("--shape", default="", help="fixed Newton kernel shape threads,lanes,pipelined (default: autotune)")
-    p.add_argument("--workload", default="batched", choices=["batched", "serve"])
+    p.add_argument("--workload", default="batched", choices=["batched", "serve", "twist"])
     p.add_argument("--rate", type=float, default=4.0, help="serve: Poisson arrival rate (requests/s)")
     p.add_argument("--duration", type=float, default=10.0, help="serve: arrival window (s)")
-    p.add_argument("--frames", type=int, default=30, help="serve: frames per request")
+    p.add_argument("--frames", type=int, default=30, help="serve: frames per request; twist: frames (0 = 300)")
+    p.add_argument("--every", type=int, default=30, help="twist: sample interval in frames")
     p.add_argument("--budget-gb", type=float, default=120.0, help="serve: device-memory budget")
     return p.parse_args()
 
@@ -499,12 +501,82 @@ def run_serve(args):
     print(json.dumps(out))
 
 
+def run_twist(args):
+    """Cable twist: 49 straight yarns (7 x 7 grid, 1.1 mm pitch) of 8192 vertices, both ends
+    pinned, the top pins rotated about the bundle axis at 2 pi rad/s by the device pin driver;
+    the FP32 production build against the FP64 build of the same kernels from identical inputs.
+    Every `--every` frames: relative position error (max difference / max displacement), the
+    largest angle between corresponding segment rotors, and the bundle twist (mean angle of
+    the yarns' mid-height vertices about the bundle axis, unwrapped) of both builds."""
+    import torch
+
+    from yarnball_b200 import scenes
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    frames = args.frames if args.frames else 300
+    every = max(1, args.every)
+    sims, centers = {}, {}
+    for prec in ("fp32", "fp64"):
+        sims[prec] = scenes.build_twist(precision=prec)
+        sims[prec].set_tuning(128, 0, True, False)
+        _, centers[prec] = scenes.device_twist(sims[prec], omega=2 * math.pi)
+    x0 = sims["fp64"].read_state_f64()[0]
+    n = sims["fp64"].numVerts
+    verts = 8192
+    mid = np.arange(49) * verts + verts // 2
+    c = centers["fp64"]
+    mid = mid[np.hypot(x0[mid, 0] - c[0], x0[mid, 2] - c[2]) > 1e-4]  # the centre yarn has no angle
+    ang0 = np.arctan2(x0[mid, 2] - c[2], x0[mid, 0] - c[0])
+
+    def twist_of(p, prev):
+        a = np.arctan2(p[mid, 2] - c[2], p[mid, 0] - c[0]) - ang0
+        a = prev + (a - prev + np.pi) % (2 * np.pi) - np.pi  # unwrap against the last sample
+        return a
+
+    def rotor_angle(q1, q2):
+        s = np.sign(np.sum(q1 * q2, axis=1, keepdims=True))
+        s[s == 0] = 1
+        return 2 * np.arctan2(np.linalg.norm(q1 - s * q2, axis=1), np.linalg.norm(q1 + s * q2, axis=1))
+
+    seg = (sims["fp64"].verts["flags"] & 2) != 0
+    rows, ms = [], {"fp32": 0.0, "fp64": 0.0}
+    tw = {"fp32": np.zeros(len(mid)), "fp64": np.zeros(len(mid))}
+    for f in range(1, frames + 1):
+        for prec in ("fp32", "fp64"):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            sims[prec].advance(FRAME)
+            e1.record()
+            e1.synchronize()
+            ms[prec] += e0.elapsed_time(e1)
+        pa, _, qa = sims["fp32"].read_state_f64()
+        pb, _, qb = sims["fp64"].read_state_f64()
+        for prec, p in (("fp32", pa), ("fp64", pb)):  # unwrapped every frame (pi per second at mid height)
+            tw[prec] = twist_of(p, tw[prec])
+        if f % every == 0 or f == frames:
+            rows.append({"frame": f, "rel_pos_err": float(np.abs(pa - pb).max() / max(np.abs(pb - x0).max(), 1e-30)),
+                         "max_rotor_angle_rad": float(rotor_angle(qa[seg], qb[seg]).max()),
+                         "twist_fp64_rad": float(tw["fp64"].mean()),
+                         "twist_err_rad": float(np.abs(tw["fp32"] - tw["fp64"]).max()),
+                         "penetrations_fp32": sims["fp32"].penetrations()})
+    for s in sims.values():
+        s.close()
+    out = {"metric": "cable twist: FP32 vs FP64 build per frame", "unit": "relative / rad", "vertices": n,
+           "frames": frames, "substeps_per_frame": SUBSTEPS, "samples": rows,
+           "throughput_vertex_substeps_per_s": {p: n * SUBSTEPS * frames / (ms[p] / 1e3) for p in ms},
+           "config": {"workload": "cable twist, 49 yarns x 8192 vertices, 2 pi rad/s, device pin driver"}}
+    print(json.dumps(out))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "serve":
         run_serve(args)
+    elif args.workload == "twist":
+        run_twist(args)
     else:
         run_ours(args)
 
