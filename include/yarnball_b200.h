@@ -324,6 +324,13 @@ yb_status yb_info(yb_sim* sim, int32_t* numVerts, int32_t* numScenes, int32_t* p
 /* Contacts with centre-line distance <= 2 * radius seen since creation (interpenetrations). */
 yb_status yb_penetration_count(yb_sim* sim, int64_t* out);
 
+/* Convergence of the Newton iteration: advances by one substep of maxH exactly as yb_step
+ * does (same schedule, same kernels in the same order, launched without a graph) and writes,
+ * for each of its Newton iterations, the largest change of the iterate over all vertices,
+ * max |dx_new - dx_old| in FP64 (metres), to maxDelta[0..min(numItr, capacity)).
+ * *numIterations receives numItr. */
+yb_status yb_step_residuals(yb_sim* sim, double* maxDelta, int32_t capacity, int32_t* numIterations);
+
 /* FP64 diagnostics of the current device state (substep start), computed on the device:
  * out[0] kinetic, out[1] gravity potential, out[2] stretch, out[3] bend, out[4] barrier
  * energy (each contact pair once), out[5] max |v|, out[6] min normalised contact gap,

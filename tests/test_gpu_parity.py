@@ -233,3 +233,44 @@ def test_upload_rejects_bad_connection_index_and_keeps_the_state():
     sim.advance(1 / 30.0)
     assert np.all(np.isfinite(sim.read_state_f64()[0]))
     sim.close()
+
+
+def _oracle_residuals(orc, h, iters):
+    """The FP64 oracle's largest iterate change per Newton iteration of one substep with
+    detection (predictor, detection and step limits, then one iteration at a time)."""
+    orc.phases(1 | 2, h)
+    prev = orc.state()["dx"][:, :3].copy()
+    out = []
+    for _ in range(iters):
+        orc.phases(16)
+        cur = orc.state()["dx"][:, :3].copy()
+        out.append(np.linalg.norm(cur - prev, axis=1).max())
+        prev = cur
+    return np.array(out)
+
+
+def test_step_residuals_is_a_plain_step():
+    """yb_step_residuals advances exactly as yb_step does (bit-exact state, same step count)
+    and reports one finite, decreasing-overall residual per Newton iteration."""
+    a = scenes.build_pile(seed=5, yarns=64, verts=64)
+    b = scenes.build_pile(seed=5, yarns=64, verts=64)
+    for _ in range(3):
+        r = a.step_residuals()
+        b.step()
+        assert len(r) == a.meta.numItr
+        assert np.all(np.isfinite(r)) and r[-1] < r[0]
+    assert a.stepCount() == b.stepCount() == 3
+    for x, y in zip(a.read_state_f64(), b.read_state_f64()):
+        assert np.array_equal(x, y)
+    a.close()
+    b.close()
+
+
+def test_step_residuals_fp64_vs_fp64_oracle():
+    """The FP64 build's per-iteration residuals equal the FP64 oracle's to 1e-8 of the first."""
+    sim = scenes.build_pile(seed=5, yarns=64, verts=64, precision="fp64")
+    orc = oracle.from_sim(sim, mode=oracle.FP64)
+    r = sim.step_residuals()
+    ref = _oracle_residuals(orc, 1e-3, len(r))
+    assert np.abs(r - ref).max() <= 1e-8 * ref[0], (r, ref)
+    sim.close()

@@ -16,4 +16,8 @@ void launch_state_f64(const Dev<R>& d, int buf, double* pos, double* vel, double
 template <typename R> void launch_scene_root_box(const Dev<R>& d, float* out, cudaStream_t s);
 // Writes 8 doubles per block into part; returns the number of blocks.
 template <typename R> int launch_diag(const Dev<R>& d, double* part, cudaStream_t s);
+// Largest change of the Newton iterate made by the last iteration (which read buffer src and
+// wrote src ^ 1), max over vertices of |dx_new - dx_old| in FP64, folded into *slot (the bit
+// pattern of a non-negative double; zero it first).
+template <typename R> void launch_iter_delta(const Dev<R>& d, int src, unsigned long long* slot, cudaStream_t s);
 }  // namespace yb

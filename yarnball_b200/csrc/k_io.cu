@@ -282,6 +282,25 @@ int launch_diag(const Dev<R>& d, double* part, cudaStream_t s) {
     return nb;
 }
 
+template <typename R>
+__global__ void __launch_bounds__(256) k_iter_delta(Dev<R> d, int src, unsigned long long* slot) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double v = 0.0;
+    if (i < d.n) {
+        const V4<R> a = d.dx[src][i].a, b = d.dx[src ^ 1][i].a;
+        const double x = (double)b.x - (double)a.x, y = (double)b.y - (double)a.y, z = (double)b.z - (double)a.z;
+        v = sqrt(x * x + y * y + z * z);
+    }
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0 && v > 0.0) atomicMax(slot, (unsigned long long)__double_as_longlong(v));
+}
+
+template <typename R>
+void launch_iter_delta(const Dev<R>& d, int src, unsigned long long* slot, cudaStream_t s) {
+    if (d.n <= 0) return;
+    k_iter_delta<R><<<(d.n + 255) / 256, 256, 0, s>>>(d, src, slot);
+}
+
 #define YB_INST(R)                                                                                          \
     template void launch_convert_in<R>(const Dev<R>&, const void*, const float*, const float*, const float*, \
                                        const int*, cudaStream_t);                                            \
@@ -292,6 +311,7 @@ int launch_diag(const Dev<R>& d, double* part, cudaStream_t s) {
     template void launch_zero_vel<R>(const Dev<R>&, cudaStream_t);                                           \
     template void launch_state_f64<R>(const Dev<R>&, int, double*, double*, double*, double*, cudaStream_t); \
     template void launch_scene_root_box<R>(const Dev<R>&, float*, cudaStream_t);                             \
+    template void launch_iter_delta<R>(const Dev<R>&, int, unsigned long long*, cudaStream_t);               \
     template int launch_diag<R>(const Dev<R>&, double*, cudaStream_t);
 YB_INST(float)
 YB_INST(double)

@@ -42,7 +42,7 @@ struct EngineBase {
     virtual yb_status download() = 0;
     virtual yb_status zero_vel() = 0;
     virtual void write_params() = 0;
-    virtual uint64_t enqueue_substep(bool detect, bool rebuild) = 0;
+    virtual uint64_t enqueue_substep(bool detect, bool rebuild, unsigned long long* slots = nullptr) = 0;
     virtual yb_status run_substep(int type) = 0;
     virtual void invalidate_graphs() = 0;
     virtual yb_status check_errors() = 0;
@@ -61,6 +61,7 @@ struct EngineBase {
     virtual yb_status save_device(FILE* f) = 0;
     virtual yb_status load_device(FILE* f) = 0;
     virtual yb_status drive_pins(double dt) = 0;
+    virtual yb_status residual_substep(int type, double* out, int cap, int* count) = 0;
 };
 
 }  // namespace
@@ -691,7 +692,9 @@ struct Engine : EngineBase {
     }
 
     // Enqueues one substep on the stream; returns the number of kernels it launches.
-    uint64_t enqueue_substep(bool detect, bool rebuild) override {
+    // One substep's kernels on S->stream; returns how many were launched.  With slots, the
+    // largest iterate change of Newton iteration it is reduced into slots[it] after it.
+    uint64_t enqueue_substep(bool detect, bool rebuild, unsigned long long* slots = nullptr) override {
         cudaStream_t st = S->stream;
         uint64_t k = 0;
         launch_init(d, st); k++;
@@ -712,6 +715,7 @@ struct Engine : EngineBase {
         for (int it = 0; it < I; it++) {
             launch_iter(d, it & 1, S->iterThreads, S->iterLanes, S->iterPipe, st);
             k++;
+            if (slots) { launch_iter_delta(d, it & 1, slots + it, st); k++; }
         }
         launch_end(d, I & 1, (I & 1) != 0, sizeof(R) == 4, st); k++;
         return k;
@@ -923,6 +927,32 @@ struct Engine : EngineBase {
         cudaEventDestroy(e1);
         *ms = t / reps;
         return cuda_status(e);
+    }
+
+    // One substep of the given shape, launched kernel by kernel (no graph) in the order of
+    // enqueue_substep, with the largest iterate change of every Newton iteration recorded.
+    yb_status residual_substep(int type, double* out, int cap, int* count) override {
+        cudaStream_t st = S->stream;
+        const bool detect = type != 2, rebuild = type == 0;
+        const int I = num_itr();
+        unsigned long long* slots = nullptr;
+        YB_CUDA(cudaMalloc(&slots, sizeof(unsigned long long) * (size_t)std::max(I, 1)));
+        cudaError_t e = cudaMemsetAsync(slots, 0, sizeof(unsigned long long) * (size_t)std::max(I, 1), st);
+        uint64_t k = 0;
+        if (e == cudaSuccess) {
+            k = enqueue_substep(detect, rebuild, slots);
+            e = cudaGetLastError();
+        }
+        std::vector<unsigned long long> h((size_t)std::max(I, 1));
+        if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), slots, sizeof(unsigned long long) * h.size(),
+                                                  cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        cudaFree(slots);
+        if (e != cudaSuccess) return cuda_status(e);
+        S->launches += k;
+        for (int it = 0; it < I && it < cap; it++) std::memcpy(out + it, &h[it], sizeof(double));
+        *count = I;
+        return YB_OK;
     }
 
     uint64_t debug_phases(int mask, int& buf) override {
@@ -1687,6 +1717,40 @@ yb_status yb_debug_dx(yb_sim* S, double* dx4) {
     if (!S || !dx4) return YB_ERR_INVALID_ARGUMENT;
     if (!S->configured) return YB_ERR_NOT_CONFIGURED;
     return S->eng->read_state_f64(nullptr, nullptr, nullptr, dx4, S->dbgBuf);
+}
+
+yb_status yb_step_residuals(yb_sim* S, double* maxDelta, int32_t capacity, int32_t* numIterations) {
+    if (!S || !numIterations || capacity < 0 || (capacity > 0 && !maxDelta)) return YB_ERR_INVALID_ARGUMENT;
+    if (!S->configured) return YB_ERR_NOT_CONFIGURED;
+    // one substep of maxH with the schedule of yb_advance (step.cpp:101-120)
+    const float dt = S->maxH;
+    for (auto& m : S->meta) {
+        m.lastH = m.h;
+        m.h = dt;
+    }
+    yb_status st = validate_all_meta(S);
+    if (st != YB_OK) return st;
+    S->eng->write_params();
+    st = S->eng->drive_pins(dt);
+    if (st != YB_OK) return st;
+    const yb_meta& m0 = S->meta[0];
+    int type = 2;
+    if (m0.detectionPeriod > 0 && S->stepCounter % (uint64_t)m0.detectionPeriod == 0) {
+        if (S->lastBVHRebuild >= m0.bvhRebuildPeriod) {
+            type = 0;
+            S->lastBVHRebuild = 0;
+        } else {
+            type = 1;
+            S->lastBVHRebuild += m0.h * m0.detectionPeriod;
+        }
+    }
+    int count = 0;
+    st = S->eng->residual_substep(type, maxDelta, capacity, &count);
+    if (st != YB_OK) return st;
+    S->stepCounter++;
+    for (auto& m : S->meta) m.time += dt;
+    *numIterations = count;
+    return S->eng->check_errors();
 }
 
 yb_status yb_debug_phases(yb_sim* S, int32_t mask, float h) {

@@ -341,6 +341,15 @@ class Sim:
         keys = ["kinetic", "gravity", "stretch", "bend", "barrier", "max_speed", "min_gap", "pairs"]
         return dict(zip(keys, out.tolist()))
 
+    def step_residuals(self):
+        """One substep of maxH (as step()) returning the largest iterate change of each Newton
+        iteration (FP64, metres)."""
+        out = np.zeros(256, np.float64)
+        cnt = ctypes.c_int32()
+        check(self._lib.yb_step_residuals(self._h, ptr(out, ctypes.c_double), len(out), ctypes.byref(cnt)),
+              "step_residuals")
+        return out[:min(cnt.value, len(out))].copy()
+
     def read_state_f64(self):
         n = self.numVerts
         pos = np.zeros((n, 3)); vel = np.zeros((n, 3)); q = np.zeros((n, 4))
