@@ -57,6 +57,7 @@ def parse():
     p.add_argument("--duration", type=float, default=10.0, help="serve: arrival window (s)")
     p.add_argument("--frames", type=int, default=30, help="serve: frames per request; twist: frames (0 = 300)")
     p.add_argument("--every", type=int, default=30, help="twist: sample interval in frames")
+    p.add_argument("--gravity", type=float, default=-9.8, help="twist: gravity along y (m/s^2)")
     p.add_argument("--budget-gb", type=float, default=120.0, help="serve: device-memory budget")
     return p.parse_args()
 
@@ -507,31 +508,38 @@ def run_twist(args):
     the FP32 production build against the FP64 build of the same kernels from identical inputs.
     Every `--every` frames: relative position error (max difference / max displacement), the
     largest angle between corresponding segment rotors, and the bundle twist (mean angle of
-    the yarns' mid-height vertices about the bundle axis, unwrapped) of both builds."""
+    the yarns' vertices at half and 0.9 of the height about the bundle axis, unwrapped) of both builds.  The run
+    stops at the first frame where either build reports an error (the reference throws on
+    MAX_COLLISIONS_PER_SEGMENT, YarnBall.cu:283-285); that frame and the largest contact count
+    per segment of every sample are reported."""
     import torch
 
-    from yarnball_b200 import scenes
+    from yarnball_b200 import YarnBallError, scenes
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     frames = args.frames if args.frames else 300
     every = max(1, args.every)
     sims, centers = {}, {}
     for prec in ("fp32", "fp64"):
-        sims[prec] = scenes.build_twist(precision=prec)
+        sims[prec] = scenes.build_twist(precision=prec, meta={"gravity": (0.0, args.gravity, 0.0)})
         sims[prec].set_tuning(128, 0, True, False)
         _, centers[prec] = scenes.device_twist(sims[prec], omega=2 * math.pi)
     x0 = sims["fp64"].read_state_f64()[0]
     n = sims["fp64"].numVerts
     verts = 8192
-    mid = np.arange(49) * verts + verts // 2
     c = centers["fp64"]
-    mid = mid[np.hypot(x0[mid, 0] - c[0], x0[mid, 2] - c[2]) > 1e-4]  # the centre yarn has no angle
-    ang0 = np.arctan2(x0[mid, 2] - c[2], x0[mid, 0] - c[0])
+    levels = {}
+    for frac in (0.5, 0.9):  # fraction of the height; the driven pins are at the top
+        idx = np.arange(49) * verts + int(frac * (verts - 1))
+        idx = idx[np.hypot(x0[idx, 0] - c[0], x0[idx, 2] - c[2]) > 1e-4]  # the centre yarn has no angle
+        levels[frac] = (idx, np.arctan2(x0[idx, 2] - c[2], x0[idx, 0] - c[0]))
 
     def twist_of(p, prev):
-        a = np.arctan2(p[mid, 2] - c[2], p[mid, 0] - c[0]) - ang0
-        a = prev + (a - prev + np.pi) % (2 * np.pi) - np.pi  # unwrap against the last sample
-        return a
+        out = {}
+        for frac, (idx, a0) in levels.items():
+            a = np.arctan2(p[idx, 2] - c[2], p[idx, 0] - c[0]) - a0
+            out[frac] = prev[frac] + (a - prev[frac] + np.pi) % (2 * np.pi) - np.pi  # unwrap against the last frame
+        return out
 
     def rotor_angle(q1, q2):
         s = np.sign(np.sum(q1 * q2, axis=1, keepdims=True))
@@ -540,32 +548,42 @@ def run_twist(args):
 
     seg = (sims["fp64"].verts["flags"] & 2) != 0
     rows, ms = [], {"fp32": 0.0, "fp64": 0.0}
-    tw = {"fp32": np.zeros(len(mid)), "fp64": np.zeros(len(mid))}
+    tw = {p: {frac: np.zeros(len(idx)) for frac, (idx, _) in levels.items()} for p in ("fp32", "fp64")}
+    stopped, done = {}, 0
     for f in range(1, frames + 1):
         for prec in ("fp32", "fp64"):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
-            sims[prec].advance(FRAME)
+            try:
+                sims[prec].advance(FRAME)
+            except YarnBallError as err:
+                stopped[prec] = {"frame": f, "error": str(err)}
             e1.record()
             e1.synchronize()
             ms[prec] += e0.elapsed_time(e1)
+        if stopped:
+            break
+        done = f
         pa, _, qa = sims["fp32"].read_state_f64()
         pb, _, qb = sims["fp64"].read_state_f64()
-        for prec, p in (("fp32", pa), ("fp64", pb)):  # unwrapped every frame (pi per second at mid height)
+        for prec, p in (("fp32", pa), ("fp64", pb)):  # unwrapped every frame
             tw[prec] = twist_of(p, tw[prec])
         if f % every == 0 or f == frames:
             rows.append({"frame": f, "rel_pos_err": float(np.abs(pa - pb).max() / max(np.abs(pb - x0).max(), 1e-30)),
                          "max_rotor_angle_rad": float(rotor_angle(qa[seg], qb[seg]).max()),
-                         "twist_fp64_rad": float(tw["fp64"].mean()),
-                         "twist_err_rad": float(np.abs(tw["fp32"] - tw["fp64"]).max()),
-                         "penetrations_fp32": sims["fp32"].penetrations()})
+                         "twist_fp64_rad": {str(fr): float(tw["fp64"][fr].mean()) for fr in levels},
+                         "twist_err_rad": {str(fr): float(np.abs(tw["fp32"][fr] - tw["fp64"][fr]).max()) for fr in levels},
+                         "penetrations_fp32": sims["fp32"].penetrations(),
+                         "max_contacts_per_segment": {p: sims[p].collisionStats()[2] for p in sims}})
     for s in sims.values():
         s.close()
     out = {"metric": "cable twist: FP32 vs FP64 build per frame", "unit": "relative / rad", "vertices": n,
-           "frames": frames, "substeps_per_frame": SUBSTEPS, "samples": rows,
-           "throughput_vertex_substeps_per_s": {p: n * SUBSTEPS * frames / (ms[p] / 1e3) for p in ms},
-           "config": {"workload": "cable twist, 49 yarns x 8192 vertices, 2 pi rad/s, device pin driver"}}
+           "frames": done, "frames_requested": frames, "stopped": stopped or None,
+           "substeps_per_frame": SUBSTEPS, "samples": rows,
+           "throughput_vertex_substeps_per_s": {p: n * SUBSTEPS * max(done, 1) / (ms[p] / 1e3) for p in ms},
+           "config": {"workload": "cable twist, 49 yarns x 8192 vertices, 2 pi rad/s, device pin driver",
+                      "gravity_y": args.gravity}}
     print(json.dumps(out))
 
 
