@@ -336,6 +336,7 @@ def run_ours(args):
 
     diag = sim.diagnostics()
     pens = sim.penetrations()
+    min_dist = sim.min_pair_distance()
     plain = None
     if not args.no_plain and rank == 0 and world == 1:
         plain = run_plain(spec, stream, (tune_threads, tune_lanes, tune_pipe))
@@ -357,7 +358,11 @@ def run_ours(args):
             "batched_over_plain": (value / plain["value"]) if plain else None,
             "contacts": {"pairs": total_pairs, "segments_with_contacts": segs_with, "max_per_segment": max_cols,
                          "cbar": cbar},
-            "interpenetrations": pens, "diagnostics": diag, "accuracy": acc,
+            # every listed contact at the start of every substep of the run (warm-up included):
+            # centre-lines crossing (distance 0) and hard cores touching (distance <= 2 radius)
+            "interpenetrations": {"min_centre_line_distance_m": min_dist, "zero_distance": int(min_dist <= 0.0),
+                                  "hard_core_contacts": pens, "two_radius_m": 2 * float(scenes.RADIUS)},
+            "diagnostics": diag, "accuracy": acc,
         }
         print(json.dumps(out))
     if dist:
@@ -575,6 +580,7 @@ def run_twist(args):
                          "twist_fp64_rad": {str(fr): float(tw["fp64"][fr].mean()) for fr in levels},
                          "twist_err_rad": {str(fr): float(np.abs(tw["fp32"][fr] - tw["fp64"][fr]).max()) for fr in levels},
                          "penetrations_fp32": sims["fp32"].penetrations(),
+                         "min_pair_distance_m": {p: sims[p].min_pair_distance() for p in sims},
                          "max_contacts_per_segment": {p: sims[p].collisionStats()[2] for p in sims}})
     for s in sims.values():
         s.close()

@@ -324,6 +324,11 @@ yb_status yb_info(yb_sim* sim, int32_t* numVerts, int32_t* numScenes, int32_t* p
 /* Contacts with centre-line distance <= 2 * radius seen since creation (interpenetrations). */
 yb_status yb_penetration_count(yb_sim* sim, int64_t* out);
 
+/* Smallest centre-line distance (metres, rounded to float) between the two segments of any
+ * listed contact, at the start of every substep since creation; +inf while no contact has
+ * been listed.  The segments' centre-lines have crossed when it reaches 0. */
+yb_status yb_min_pair_distance(yb_sim* sim, double* out);
+
 /* Convergence of the Newton iteration: advances by one substep of maxH exactly as yb_step
  * does (same schedule, same kernels in the same order, launched without a graph) and writes,
  * for each of its Newton iterations, the largest change of the iterate over all vertices,

@@ -274,3 +274,28 @@ def test_step_residuals_fp64_vs_fp64_oracle():
     ref = _oracle_residuals(orc, 1e-3, len(r))
     assert np.abs(r - ref).max() <= 1e-8 * ref[0], (r, ref)
     sim.close()
+
+
+def test_min_pair_distance_is_the_listed_minimum():
+    """The running minimum of the contacts' centre-line distances equals an FP64 evaluation
+    over the listed contacts (within 1e-7 m: FP32 relative coordinates), and starts at +inf."""
+    from tests.np_ref import closest
+
+    sim = scenes.build_pile(seed=9, yarns=96, verts=64, cube=0.03)
+    assert sim.min_pair_distance() == np.inf
+    sim.debug_phases(1 | 2, H)
+    pos = sim.read_state_f64()[0]
+    nc, lists, _ = sim.debug_contacts()
+    best = np.inf
+    for i in np.nonzero(nc)[0]:
+        a0 = pos[i]
+        a1 = pos[i + 1] - a0
+        for j in lists[i]:
+            b0, b1 = pos[j] - a0, pos[j + 1] - a0
+            u, v = closest(a1, b0, b1)
+            best = min(best, float(np.linalg.norm(u * a1 - (b0 * (1 - v) + b1 * v))))
+    got = sim.min_pair_distance()
+    assert np.isfinite(best) and abs(got - best) <= 1e-7, (got, best)
+    sim.advance(1 / 30.0)
+    assert 0.0 < sim.min_pair_distance() <= got
+    sim.close()

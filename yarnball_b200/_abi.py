@@ -140,6 +140,7 @@ SIGNATURES = {
     "yb_penetration_count": (ctypes.c_int, [_P, c_int64_p]),
     "yb_diagnostics": (ctypes.c_int, [_P, c_double_p]),
     "yb_step_residuals": (ctypes.c_int, [_P, c_double_p, ctypes.c_int32, c_int32_p]),
+    "yb_min_pair_distance": (ctypes.c_int, [_P, c_double_p]),
     "yb_read_state_f64": (ctypes.c_int, [_P, c_double_p, c_double_p, c_double_p]),
     "yb_debug_contacts": (ctypes.c_int, [_P, c_int32_p, c_int32_p, c_float_p]),
     "yb_debug_dx": (ctypes.c_int, [_P, c_double_p]),

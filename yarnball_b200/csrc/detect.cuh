@@ -74,8 +74,9 @@ __device__ __forceinline__ bool pair_keep(const Dev<R>& d, int x, int y, const S
 // Step-size limit (collision.cu:121-159), split so that contacts can be spread over threads:
 // step_limit_base is the per-segment start value, contact_step_limit one contact's bound
 // 0.45 x centre-line distance.  A contact also stages the partner's endpoints relative to p0
-// (for c < RELCAP, read by every Newton iteration of the substep) and reports an
-// interpenetration (distance at or below 2 radius, each unordered pair once, o > k).
+// (for c < RELCAP, read by every Newton iteration of the substep), reports an
+// interpenetration (distance at or below 2 radius, each unordered pair once, o > k) and
+// returns the centre-line distance in dist.
 template <typename R>
 __device__ __forceinline__ R step_limit_base(const Dev<R>& d, int k, const SceneParams<R>& sp) {
     typedef Ex<R> E;
@@ -86,7 +87,7 @@ __device__ __forceinline__ R step_limit_base(const Dev<R>& d, int k, const Scene
 
 template <typename R>
 __device__ __forceinline__ R contact_step_limit(const Dev<R>& d, int k, int c, int o, const V3<R>& a0,
-                                                const V3<R>& a1, const SceneParams<R>& sp, bool& pen) {
+                                                const V3<R>& a1, const SceneParams<R>& sp, bool& pen, R& dist) {
     typedef Ex<R> E;
     const V3<R> b0 = xsub(xyz(d.pos[o]), a0);
     const V3<R> b1 = xsub(xyz(d.pos[o + 1]), a0);
@@ -102,6 +103,7 @@ __device__ __forceinline__ R contact_step_limit(const Dev<R>& d, int k, int c, i
     const V3<R> nrm = xsub(xscale(uv.u, a1), xmix(b0, b1, uv.v));
     const R l = E::sqrt(xlen2(nrm));
     pen = o > k && l <= sp.twoR;
+    dist = l;
     const R safe = E::mul(E::sub(R(1), R(0.1f)), R(0.5f));
     return E::mul(safe, l);
 }

@@ -39,6 +39,8 @@ enum {
     EW_INTERNAL = 2,     // bit mask of IE_* below
     EW_PENETRATIONS = 3, // number of contacts seen with distance <= 2 * radius (cumulative)
     EW_MAX_COLS = 4,     // largest contact count of any segment (cumulative max)
+    EW_MIN_DIST = 5,     // float bits of the smallest centre-line distance of any listed contact
+                         // at substep start (cumulative min; +inf before the first contact)
     EW_COUNT = 8
 };
 enum { IE_BVH_STACK = 1, IE_SORT_WAIT = 2, IE_GRID_WAIT = 4, IE_REFIT = 8 };

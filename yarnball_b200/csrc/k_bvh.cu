@@ -495,6 +495,7 @@ __global__ void __launch_bounds__(128) k_lists(Dev<R> d, int sortLists) {
     R m = R(0);
     if (valid) m = step_limit_base(d, k, d.sp[sc]);
     int pens = 0;
+    float dmin = INFINITY;
     for (int base = 0; base < total; base += B) {
         const int f = base + t;
         R lim = yinf<R>();
@@ -510,8 +511,10 @@ __global__ void __launch_bounds__(128) k_lists(Dev<R> d, int sortLists) {
             const V3<R> oa0(sA0[0][s], sA0[1][s], sA0[2][s]);
             const V3<R> oa1(sA1[0][s], sA1[1][s], sA1[2][s]);
             bool pen = false;
-            lim = contact_step_limit(d, ks, c, o, oa0, oa1, d.sp[sScene[s]], pen);
+            R dist;
+            lim = contact_step_limit(d, ks, c, o, oa0, oa1, d.sp[sScene[s]], pen, dist);
             pens += pen;
+            dmin = fminf(dmin, (float)dist);
         }
         sLim[t] = lim;
         __syncthreads();
@@ -523,6 +526,10 @@ __global__ void __launch_bounds__(128) k_lists(Dev<R> d, int sortLists) {
         atomicAdd(&d.err[EW_PENETRATIONS], pens);
         d.err[EW_WARNING] = 2;
     }
+    // distances are >= 0, whose float bit patterns order like the integers
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dmin = fminf(dmin, __shfl_xor_sync(0xffffffffu, dmin, o));
+    if ((t & 31) == 0 && dmin < INFINITY) atomicMin(&d.err[EW_MIN_DIST], __float_as_int(dmin));
     if (valid) d.stepLim[k] = d.sp[sc].useStepLimit ? m : yinf<R>();
 }
 

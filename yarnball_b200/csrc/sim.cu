@@ -52,6 +52,7 @@ struct EngineBase {
     virtual yb_status diagnostics(double* out) = 0;
     virtual uint64_t debug_phases(int mask, int& buf) = 0;
     virtual int64_t penetrations() = 0;
+    virtual double min_distance() = 0;
     virtual yb_status profile_substep(bool detect, bool rebuild, double* ms, uint64_t* launches) = 0;
     virtual yb_status time_iter(int threads, int lanes, int pipe, int reps, float* ms) = 0;
     virtual yb_status download_range(int first, int count) = 0;
@@ -304,6 +305,7 @@ struct Engine : EngineBase {
     int graphItr = -1, graphThreads = -1, graphLanes = -1, graphPipe = -1, graphNseg = -1;
     int keyBits = 30;
     int64_t penTotal = 0;
+    float minDist = INFINITY;
 
     explicit Engine(yb_sim* s) : S(s) {}
 
@@ -385,6 +387,8 @@ struct Engine : EngineBase {
         YB_CUDA(cudaHostAlloc((void**)&spHost, sizeof(SceneParams<R>) * ns, cudaHostAllocDefault));
         YB_CUDA(cudaHostAlloc((void**)&errHost, sizeof(int) * EW_COUNT, cudaHostAllocDefault));
         YB_CUDA(cudaMemsetAsync(d.err, 0, sizeof(int) * EW_COUNT, S->stream));
+        static const int kInfBits = 0x7f800000;  // EW_MIN_DIST starts at +inf
+        YB_CUDA(cudaMemcpyAsync(d.err + EW_MIN_DIST, &kInfBits, sizeof(int), cudaMemcpyHostToDevice, S->stream));
         YB_CUDA(cudaMemsetAsync(d.numCols, 0, sizeof(int) * n, S->stream));
         YB_CUDA(cudaMemsetAsync(d.lastVel, 0, sizeof(V4<R>) * n, S->stream));
         YB_CUDA(cudaMemsetAsync(d.refitCount, 0, sizeof(unsigned) * nn, S->stream));
@@ -769,6 +773,7 @@ struct Engine : EngineBase {
         YB_CUDA(cudaStreamSynchronize(S->stream));
         yb_status st = YB_OK;
         penTotal = errHost[EW_PENETRATIONS];
+        std::memcpy(&minDist, &errHost[EW_MIN_DIST], sizeof(float));
         if (errHost[EW_ERROR] != 0) {
             S->lastErrorCode = errHost[EW_ERROR];
             st = YB_ERR_MAX_COLLISIONS_PER_SEGMENT_EXCEEDED;
@@ -781,6 +786,7 @@ struct Engine : EngineBase {
     }
 
     int64_t penetrations() override { return penTotal; }
+    double min_distance() override { return minDist; }
 
     yb_status read_state_f64(double* pos, double* vel, double* q, double* dx, int buf) override {
         const size_t n = (size_t)S->n;
@@ -1692,6 +1698,14 @@ yb_status yb_penetration_count(yb_sim* S, int64_t* out) {
     if (!S->configured) return YB_ERR_NOT_CONFIGURED;
     const yb_status st = S->eng->check_errors();
     *out = S->eng->penetrations();
+    return st == YB_ERR_MAX_COLLISIONS_PER_SEGMENT_EXCEEDED ? YB_OK : st;
+}
+
+yb_status yb_min_pair_distance(yb_sim* S, double* out) {
+    if (!S || !out) return YB_ERR_INVALID_ARGUMENT;
+    if (!S->configured) return YB_ERR_NOT_CONFIGURED;
+    const yb_status st = S->eng->check_errors();
+    *out = S->eng->min_distance();
     return st == YB_ERR_MAX_COLLISIONS_PER_SEGMENT_EXCEEDED ? YB_OK : st;
 }
 

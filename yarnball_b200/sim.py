@@ -334,6 +334,12 @@ class Sim:
         check(self._lib.yb_penetration_count(self._h, ctypes.byref(v)))
         return int(v.value)
 
+    def min_pair_distance(self):
+        """Smallest centre-line distance (m) of any listed contact at substep start since creation."""
+        v = ctypes.c_double()
+        check(self._lib.yb_min_pair_distance(self._h, ctypes.byref(v)), "min_pair_distance")
+        return v.value
+
     def diagnostics(self):
         """FP64 energies and contact statistics of the device state (see yarnball_b200.h)."""
         out = np.zeros(8, np.float64)
