@@ -188,7 +188,9 @@ yb_status yb_get_tuning(yb_sim* sim, int32_t* iterThreads, int32_t* lanesPerVert
                         int32_t* useGraphs);
 
 /* Autotuner: times every Newton-kernel shape on the current device state (which it leaves
- * unchanged), keeps the fastest and returns it.  Call after at least one advance(). */
+ * unchanged; three interleaved rounds of 8 launches per shape, each shape's fastest round),
+ * keeps the fastest and returns it with its time per launch.  Call after at least one
+ * advance(). */
 yb_status yb_autotune(yb_sim* sim, int32_t* bestThreads, int32_t* bestLanes, int32_t* bestPipelined,
                       float* bestMs);
 

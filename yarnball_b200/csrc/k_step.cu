@@ -398,9 +398,9 @@ __global__ void __launch_bounds__(NT, MINB) k_iter(Dev<R> d, int src) {
 // B segments are flattened (block scan of the counts); every thread takes contacts
 // f = tid, tid + B, ... of the flattened list, so a warp never waits for its longest list and
 // the partner gathers of the whole block are in flight together.  Each thread writes its
-// contact's 18-value contribution to shared memory; the owning segment then adds its
-// contacts in list order, so the result is deterministic.  The rest (own terms, vertex
-// solve, orientation update) is k_iter's.
+// contact's 18-value contribution to shared memory (four 16-byte and one 8-byte store); the
+// owning segment then adds its contacts in list order, so the result is deterministic.  The
+// rest (own terms, vertex solve, orientation update) is k_iter's.
 template <typename R, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) k_iter_bal(Dev<R> d, int src) {
     constexpr int B = NT;
@@ -414,7 +414,10 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_bal(Dev<R> d, int src) {
     const V4<R>* __restrict__ QO = d.q[src];
 
     __shared__ R sSeg[12][B];  // p0, e = p1 - p0, dx, dx1 of each slot's segment
-    __shared__ R sCon[2][18][B];  // contributions of one chunk of contacts (double buffered)
+    // contributions of one chunk of contacts, double buffered, in 16-byte groups:
+    // (fa, fb.x) (fb.yz, Ha0-1) (Ha2-5) (Hb0-3), then (Hb4-5)
+    __shared__ V4<R> sCon4[2][4][B];
+    __shared__ R2<R> sCon2[2][B];
     __shared__ int sOwn[2][B];     // owning slot of each contact of a chunk (double buffered)
     __shared__ int sOff[B + 1];
     __shared__ int sScene[B];
@@ -511,34 +514,39 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_bal(Dev<R> d, int src) {
             const V3<R> sdx1(sSeg[9][s], sSeg[10][s], sSeg[11][s]);
             contact_term(se, sdx, sdx1, r0, r1, xyz(pd.a), xyz(pd.b), d.sp[sScene[s]], cfa, cHa, cfb, cHb);
         }
-        R (*con)[B] = sCon[buf];
-        con[0][t] = cfa.x; con[1][t] = cfa.y; con[2][t] = cfa.z;
-        con[3][t] = cfb.x; con[4][t] = cfb.y; con[5][t] = cfb.z;
-#pragma unroll
-        for (int q = 0; q < 6; q++) {
-            con[6 + q][t] = cHa.d[q];
-            con[12 + q][t] = cHb.d[q];
+        {
+            V4<R> w;
+            w.x = cfa.x; w.y = cfa.y; w.z = cfa.z; w.w = cfb.x; sCon4[buf][0][t] = w;
+            w.x = cfb.y; w.y = cfb.z; w.z = cHa.d[0]; w.w = cHa.d[1]; sCon4[buf][1][t] = w;
+            w.x = cHa.d[2]; w.y = cHa.d[3]; w.z = cHa.d[4]; w.w = cHa.d[5]; sCon4[buf][2][t] = w;
+            w.x = cHb.d[0]; w.y = cHb.d[1]; w.z = cHb.d[2]; w.w = cHb.d[3]; sCon4[buf][3][t] = w;
+            R2<R> w2;
+            w2.x = cHb.d[4]; w2.y = cHb.d[5];
+            sCon2[buf][t] = w2;
         }
         __syncthreads();
         const int f0 = max(myOff, base), f1 = min(myOff + nc, base + NT);
         for (int g = f0; g < f1; g++) {
             const int i = g - base;
-            fa += V3<R>(con[0][i], con[1][i], con[2][i]);
-            fb += V3<R>(con[3][i], con[4][i], con[5][i]);
-#pragma unroll
-            for (int q = 0; q < 6; q++) {
-                Ha.d[q] += con[6 + q][i];
-                Hb.d[q] += con[12 + q][i];
-            }
+            const V4<R> w0 = sCon4[buf][0][i], w1 = sCon4[buf][1][i], w2 = sCon4[buf][2][i], w3 = sCon4[buf][3][i];
+            const R2<R> w4 = sCon2[buf][i];
+            fa += V3<R>(w0.x, w0.y, w0.z);
+            fb += V3<R>(w0.w, w1.x, w1.y);
+            Ha.d[0] += w1.z; Ha.d[1] += w1.w;
+            Ha.d[2] += w2.x; Ha.d[3] += w2.y; Ha.d[4] += w2.z; Ha.d[5] += w2.w;
+            Hb.d[0] += w3.x; Hb.d[1] += w3.y; Hb.d[2] += w3.z; Hb.d[3] += w3.w;
+            Hb.d[4] += w4.x; Hb.d[5] += w4.y;
         }
     }
 
     // The halo exchange after the loop uses the contribution buffer the last chunk did not
-    // use (buf): every thread finished reading it before the last chunk's barrier.
-    R (*sFb)[B] = sCon[buf];       // rows 0-2
-    R (*sHb)[B] = sCon[buf] + 3;   // rows 3-8
-    R* sSL = sCon[buf][9];
-    R (*sDX)[B] = sCon[buf] + 10;  // rows 10-12
+    // use (buf), viewed as 16 rows of B values: every thread finished reading it before the
+    // last chunk's barrier.
+    R (*rows)[B] = reinterpret_cast<R (*)[B]>(&sCon4[buf][0][0]);
+    R (*sFb)[B] = rows;       // rows 0-2
+    R (*sHb)[B] = rows + 3;   // rows 3-8
+    R* sSL = rows[9];
+    R (*sDX)[B] = rows + 10;  // rows 10-12
 
     // the vertex's own terms (cosserat.cu:40-81)
     R sl = yinf<R>();

@@ -1344,18 +1344,29 @@ yb_status yb_autotune(yb_sim* S, int32_t* bestThreads, int32_t* bestLanes, int32
     if (!S->configured) return YB_ERR_NOT_CONFIGURED;
     static const int shapes[][3] = {{256, 1, 0}, {128, 1, 0}, {256, 2, 0}, {256, 4, 0}, {512, 4, 0}, {256, 8, 0},
                                     {512, 8, 0}, {128, 1, 1}, {256, 1, 1}, {256, 4, 1}, {128, 0, 0}, {128, 0, 1}};
+    constexpr int NS = sizeof(shapes) / sizeof(shapes[0]);
     float best = INFINITY;
     int bt = S->iterThreads, bl = S->iterLanes, bp = S->iterPipe;
     S->eng->write_params();
-    for (const auto& sh : shapes) {
-        float ms = 0.f;
-        const yb_status st = S->eng->time_iter(sh[0], sh[1], sh[2], 5, &ms);
-        if (st != YB_OK) return st;
-        if (ms < best) {
-            best = ms;
-            bt = sh[0];
-            bl = sh[1];
-            bp = sh[2];
+    // Three rounds over all shapes (8 timed launches each), keeping each shape's fastest
+    // round: interleaving the rounds cancels drift, and the minimum discards launches that
+    // another stream or a clock change slowed down.
+    float shapeMs[NS];
+    for (int i = 0; i < NS; i++) shapeMs[i] = INFINITY;
+    for (int round = 0; round < 3; round++) {
+        for (int i = 0; i < NS; i++) {
+            float ms = 0.f;
+            const yb_status st = S->eng->time_iter(shapes[i][0], shapes[i][1], shapes[i][2], 8, &ms);
+            if (st != YB_OK) return st;
+            shapeMs[i] = std::min(shapeMs[i], ms);
+        }
+    }
+    for (int i = 0; i < NS; i++) {
+        if (shapeMs[i] < best) {
+            best = shapeMs[i];
+            bt = shapes[i][0];
+            bl = shapes[i][1];
+            bp = shapes[i][2];
         }
     }
     const yb_status st = yb_set_tuning(S, bt, bl, bp, S->useGraphs);
