@@ -482,6 +482,13 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_bal(Dev<R> d, int src) {
     for (int g = myOff; g < min(myOff + nc, NT); g++) sOwn[0][g] = t;
     __syncthreads();
     int buf = 0;
+    // The partner id of this thread's contact is loaded one chunk ahead (after the previous
+    // chunk's barrier, before its summation), so a chunk starts with the partner gather.
+    int jn = 0;
+    if (t < total) {
+        const int s = sOwn[0][t];
+        jn = __ldg(d.cols + col_at(blockIdx.x * CORE - 1 + s, t - sOff[s]));
+    }
     for (int base = 0; base < total; base += NT, buf ^= 1) {
         const int f = base + t;
         {
@@ -496,7 +503,7 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_bal(Dev<R> d, int src) {
             const int s = sOwn[buf][t], c = f - sOff[s];
             const int ks = blockIdx.x * CORE - 1 + s;
             const size_t at = rel_at(ks, c);
-            const int j = __ldg(d.cols + col_at(ks, c));
+            const int j = jn;
             const V3<R> sp0(sSeg[0][s], sSeg[1][s], sSeg[2][s]);
             V3<R> r0, r1;
             if (c < RELCAP) {
@@ -525,6 +532,19 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_bal(Dev<R> d, int src) {
             sCon2[buf][t] = w2;
         }
         __syncthreads();
+        {
+            // next chunk: partner id, and the staged partner positions into L1
+            const int fn = base + NT + t;
+            if (fn < total) {
+                const int s = sOwn[buf ^ 1][t], c = fn - sOff[s];
+                const int ks = blockIdx.x * CORE - 1 + s;
+                jn = __ldg(d.cols + col_at(ks, c));
+                if (c < RELCAP) {
+                    prefetch_l1(d.relA + rel_at(ks, c));
+                    prefetch_l1(d.relB + rel_at(ks, c));
+                }
+            }
+        }
         const int f0 = max(myOff, base), f1 = min(myOff + nc, base + NT);
         for (int g = f0; g < f1; g++) {
             const int i = g - base;
