@@ -299,3 +299,17 @@ def test_min_pair_distance_is_the_listed_minimum():
     sim.advance(1 / 30.0)
     assert 0.0 < sim.min_pair_distance() <= got
     sim.close()
+
+
+def test_stored_contact_lists_are_sorted():
+    """The list pass sorts every contact list in place (by its thread up to 16 entries, by
+    its warp beyond): on the full pile, with lists of more than 16 entries, every stored list
+    is strictly increasing and the pair set is that of the FP32 oracle."""
+    sim = scenes.build_pile(seed=1)
+    orc = oracle.from_sim(sim, mode=oracle.FP32_MIXED)
+    _compare_detection(sim, orc)
+    nc, lists, _ = sim.debug_contacts(raw=True)
+    assert nc.max() > 16
+    for i in np.nonzero(nc)[0]:
+        assert np.all(np.diff(lists[i]) > 0), i
+    sim.close()

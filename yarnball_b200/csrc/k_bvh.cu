@@ -426,6 +426,93 @@ __global__ void __launch_bounds__(TRAV_THREADS) k_traverse(Dev<R> d) {
     }
 }
 
+// Sorts segment k's contact list (n <= MAX_COLS distinct partner ids) ascending, in place.
+// Called by all 32 lanes of a warp (k < 0 or n = 0 for lanes without a list).  A list of up to
+// 16 entries is sorted by its own thread with a bitonic network on 16 registers; a longer one
+// by the whole warp, one list at a time, as a bitonic sort of 128 entries held four per lane
+// (entry i = 32 r + lane): steps with a stride of 32 or more swap within a lane, smaller ones
+// exchange between lanes.  Padding entries are INT_MAX and sort to the end.
+template <typename R>
+__device__ __forceinline__ void sort_list(const Dev<R>& d, int k, int n) {
+    constexpr int PAD = 0x7fffffff;
+    const int lane = threadIdx.x & 31;
+    if (k >= 0 && n > 1 && n <= 16) {
+        int* __restrict__ cl = d.cols + col_at(k, 0);
+        int v[16];
+#pragma unroll
+        for (int a = 0; a < 16; a++) v[a] = a < n ? cl[a] : PAD;
+#pragma unroll
+        for (int sz = 2; sz <= 16; sz <<= 1) {
+#pragma unroll
+            for (int st = sz >> 1; st > 0; st >>= 1) {
+#pragma unroll
+                for (int a = 0; a < 16; a++) {
+                    const int b = a ^ st;
+                    if (b > a) {
+                        const bool up = (a & sz) == 0;
+                        const int x = v[a], y = v[b];
+                        const bool sw = up ? (x > y) : (x < y);
+                        v[a] = sw ? y : x;
+                        v[b] = sw ? x : y;
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < 16; a++)
+            if (a < n) cl[a] = v[a];
+    }
+    unsigned longLists = __ballot_sync(0xffffffffu, k >= 0 && n > 16);
+    while (longLists) {
+        const int src = __ffs(longLists) - 1;
+        longLists &= longLists - 1;
+        const int kk = __shfl_sync(0xffffffffu, k, src);
+        const int m = __shfl_sync(0xffffffffu, n, src);
+        int* __restrict__ cl = d.cols + col_at(kk, 0);
+        int v[4];
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            const int i = 32 * r + lane;
+            v[r] = i < m ? cl[i] : PAD;
+        }
+#pragma unroll
+        for (int sz = 2; sz <= 128; sz <<= 1) {
+#pragma unroll
+            for (int st = sz >> 1; st > 0; st >>= 1) {
+                if (st >= 32) {
+                    const int rs = st >> 5;
+#pragma unroll
+                    for (int r = 0; r < 4; r++) {
+                        if (r & rs) continue;
+                        const int r2 = r | rs;
+                        const bool up = ((32 * r + lane) & sz) == 0;
+                        const int x = v[r], y = v[r2];
+                        const bool sw = up ? (x > y) : (x < y);
+                        v[r] = sw ? y : x;
+                        v[r2] = sw ? x : y;
+                    }
+                } else {
+#pragma unroll
+                    for (int r = 0; r < 4; r++) {
+                        const int i = 32 * r + lane;
+                        const int x = v[r];
+                        const int y = __shfl_xor_sync(0xffffffffu, x, st);
+                        const bool up = (i & sz) == 0;
+                        const bool lower = (i & st) == 0;  // the lower index of the pair
+                        v[r] = (lower == up) ? min(x, y) : max(x, y);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            const int i = 32 * r + lane;
+            if (i < m) cl[i] = v[r];
+        }
+        __syncwarp();
+    }
+}
+
 // Per segment after the broadphase: clamp and check the count, sort the list by partner id
 // (fixed summation order in the Newton iteration), then the step-size limit.  With
 // sortLists = 0 it only recomputes the step limit from the existing lists (substeps without
@@ -455,21 +542,12 @@ __global__ void __launch_bounds__(128) k_lists(Dev<R> d, int sortLists) {
             if (nc > MAX_COLS) d.err[EW_ERROR] = 1;
             if (nc) atomicMax(&d.err[EW_MAX_COLS], nc);
             nc = min(nc, MAX_COLS);
-            int* __restrict__ cl = d.cols + col_at(k, 0);
-            for (int a = 1; a < nc; a++) {
-                const int v = cl[a];
-                int b = a - 1;
-                while (b >= 0 && cl[b] > v) {
-                    cl[b + 1] = cl[b];
-                    b--;
-                }
-                cl[b + 1] = v;
-            }
             d.numCols[k] = nc;
         }
         a0 = xyz(d.pos[k]);
         a1 = xsub(xyz(d.pos[k + 1]), a0);
     }
+    if (sortLists) sort_list(d, k, valid ? nc : 0);
     sSeg[t] = k;
     sScene[t] = sc;
     sA0[0][t] = a0.x; sA0[1][t] = a0.y; sA0[2][t] = a0.z;

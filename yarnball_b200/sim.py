@@ -363,7 +363,8 @@ class Sim:
                                           ptr(q, ctypes.c_double)), "read_state")
         return pos, vel, q
 
-    def debug_contacts(self):
+    def debug_contacts(self, raw=False):
+        """(numCols, lists, stepLimit); each list sorted here, or as stored with raw=True."""
         n = self.numVerts
         nc = np.zeros(n, np.int32)
         cols = np.zeros(n * MAX_COLLISIONS_PER_SEGMENT, np.int32)
@@ -371,7 +372,8 @@ class Sim:
         check(self._lib.yb_debug_contacts(self._h, ptr(nc, ctypes.c_int32), ptr(cols, ctypes.c_int32),
                                           ptr(sl, ctypes.c_float)), "contacts")
         rows = cols.reshape(n, MAX_COLLISIONS_PER_SEGMENT)
-        lists = [np.sort(rows[i, :nc[i]]) if nc[i] else np.zeros(0, np.int32) for i in range(n)]
+        lists = [(rows[i, :nc[i]].copy() if raw else np.sort(rows[i, :nc[i]])) if nc[i] else np.zeros(0, np.int32)
+                 for i in range(n)]
         return nc, lists, sl
 
     def debug_dx(self):
