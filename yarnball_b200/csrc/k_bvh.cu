@@ -532,22 +532,29 @@ __global__ void __launch_bounds__(128) k_lists(Dev<R> d, int sortLists) {
     const int t = threadIdx.x;
     const int si = blockIdx.x * B + t;
     const bool valid = si < d.nseg;
-    int k = -1, nc = 0, sc = 0;
+    int k = -1, nc = 0, sc = 0, rawCount = 0;
     V3<R> a0(R(0)), a1(R(0));
     if (valid) {
         k = d.segs[si];
         sc = scene_of(d.vp[k].flags);
         nc = d.numCols[k];
+        rawCount = nc;
         if (sortLists) {
             if (nc > MAX_COLS) d.err[EW_ERROR] = 1;
-            if (nc) atomicMax(&d.err[EW_MAX_COLS], nc);
             nc = min(nc, MAX_COLS);
             d.numCols[k] = nc;
         }
         a0 = xyz(d.pos[k]);
         a1 = xsub(xyz(d.pos[k + 1]), a0);
     }
-    if (sortLists) sort_list(d, k, valid ? nc : 0);
+    if (sortLists) {
+        // largest list of the warp (before the clamp), one atomic per warp
+        int m = rawCount;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if ((t & 31) == 0 && m) atomicMax(&d.err[EW_MAX_COLS], m);
+        sort_list(d, k, valid ? nc : 0);
+    }
     sSeg[t] = k;
     sScene[t] = sc;
     sA0[0][t] = a0.x; sA0[1][t] = a0.y; sA0[2][t] = a0.z;
