@@ -60,6 +60,13 @@ struct alignas(sizeof(R) * 2) R2 {
 
 constexpr int RELCAP = 8;  // contacts per segment with staged relative partner positions
 
+// Wide records are built only for the nodes the walk loads: those at an even depth below
+// their scene's root (a record's entries are grandchildren).  Depths come from pointer jumping
+// over the parent links at rebuild (DEPTH_ROUNDS rounds: depths below 2^DEPTH_ROUNDS); a
+// deeper tree gets every record.
+constexpr int DEPTH_ROUNDS = 7;
+constexpr int DEPTH_LAUNCHES = 1 + DEPTH_ROUNDS + 1;  // init, jumps, marks
+
 // Contact-list addressing: each segment owns a row of MAX_COLS partner ids and a row of RELCAP
 // staged partner positions, so the contacts of one segment are contiguous (the flattened
 // contact loop of the Newton kernel reads consecutive contacts of one owner together).
@@ -149,6 +156,10 @@ struct Dev {
     // BVH
     BNode<R>* nodes;  // nseg - 1 internal nodes
     WNode<R>* wide;   // nseg - 1 wide nodes (rebuilt after every refit)
+    int* depJump[2];  // rebuild scratch: pointer-jumping parent links and distances
+    int* depDist[2];
+    unsigned char* wideUsed;  // 1: the walk can load this node's record
+    int* wideAll;     // 1: build every record (tree too deep for the depth marks)
     QRec<R>* qrec;    // per sorted leaf: box, segment, scene (written by the refit)
     int* nodeLast;    // sorted position of the last leaf of each internal node's range
     int* leafParent;  // per sorted leaf position

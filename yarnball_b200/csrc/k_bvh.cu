@@ -227,6 +227,48 @@ __global__ void __launch_bounds__(256) k_refit(Dev<R> d, const int* __restrict__
     }
 }
 
+// Depth marks for the wide records (rebuild).  Pointer jumping: after round r every node
+// knows its distance to the ancestor 2^r levels up (or to the root, with link -1).  A node's
+// record is used when its depth below its scene's root is even; a link left after the last
+// round (a tree 2^DEPTH_ROUNDS deep or more) makes every record built.
+template <typename R>
+__global__ void __launch_bounds__(256) k_depth_init(Dev<R> d) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.nseg - 1) return;
+    const int p = d.nodes[i].parent;
+    d.depJump[0][i] = p;
+    d.depDist[0][i] = p >= 0 ? 1 : 0;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_depth_jump(Dev<R> d, int src) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.nseg - 1) return;
+    const int j = d.depJump[src][i];
+    int dist = d.depDist[src][i], jj = -1;
+    if (j >= 0) {
+        dist += d.depDist[src][j];
+        jj = d.depJump[src][j];
+    }
+    d.depDist[src ^ 1][i] = dist;
+    d.depJump[src ^ 1][i] = jj;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_depth_mark(Dev<R> d, int fin) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.nseg - 1) return;
+    if (d.depJump[fin][i] >= 0) *d.wideAll = 1;
+    // internal node i's leaf range has leaf i at one end, so leaf i's key names its scene
+    const int root = d.sceneRoot[(int)(d.keys[0][i] >> 30)];
+    int used = 0;
+    if (root >= 0) {
+        const int rel = d.depDist[fin][i] - d.depDist[fin][root];
+        used = rel >= 0 && (rel & 1) == 0;
+    }
+    d.wideUsed[i] = (unsigned char)used;
+}
+
 // Wide nodes from the refitted binary tree: node i's entries are the children of its two
 // children (a leaf child is an entry itself), so a walk over wide nodes loads one node per
 // two binary levels.  Entry order: left child's left, left child's right, right child's left,
@@ -235,6 +277,7 @@ template <typename R>
 __global__ void __launch_bounds__(256) k_widen(Dev<R> d) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= d.nseg - 1) return;
+    if (!d.wideUsed[i] && !*d.wideAll) return;  // a record the walk never loads
     const BNode<R> nd = d.nodes[i];
     WNode<R> w;
     int e = 0;
@@ -634,6 +677,12 @@ void launch_bvh_rebuild(const Dev<R>& d, cudaStream_t s, void* sortScratch, size
         cudaMemcpyAsync(d.vals[0], d.vals[1], sizeof(int) * d.nseg, cudaMemcpyDeviceToDevice, s);
     }
     k_karras<R><<<nb, 256, 0, s>>>(d, d.keys[0], d.vals[0]);
+    // DEPTH_LAUNCHES kernels: which wide records the walk can load
+    const int ib = (max(d.nseg - 1, 1) + 255) / 256;
+    cudaMemsetAsync(d.wideAll, 0, sizeof(int), s);
+    k_depth_init<R><<<ib, 256, 0, s>>>(d);
+    for (int r = 0; r < DEPTH_ROUNDS; r++) k_depth_jump<R><<<ib, 256, 0, s>>>(d, r & 1);
+    k_depth_mark<R><<<ib, 256, 0, s>>>(d, DEPTH_ROUNDS & 1);
     launch_bvh_refit(d, s);
 }
 

@@ -348,6 +348,12 @@ struct Engine : EngineBase {
         want((void**)&d.err, sizeof(int) * EW_COUNT);
         want((void**)&d.nodes, sizeof(BNode<R>) * nn);
         want((void**)&d.wide, sizeof(WNode<R>) * nn);
+        want((void**)&d.depJump[0], sizeof(int) * nn);
+        want((void**)&d.depJump[1], sizeof(int) * nn);
+        want((void**)&d.depDist[0], sizeof(int) * nn);
+        want((void**)&d.depDist[1], sizeof(int) * nn);
+        want((void**)&d.wideUsed, nn);
+        want((void**)&d.wideAll, sizeof(int));
         want((void**)&d.qrec, sizeof(QRec<R>) * n);
         want((void**)&d.nodeLast, sizeof(int) * nn);
         want((void**)&d.leafParent, sizeof(int) * n);
@@ -392,6 +398,13 @@ struct Engine : EngineBase {
         YB_CUDA(cudaMemsetAsync(d.numCols, 0, sizeof(int) * n, S->stream));
         YB_CUDA(cudaMemsetAsync(d.lastVel, 0, sizeof(V4<R>) * n, S->stream));
         YB_CUDA(cudaMemsetAsync(d.refitCount, 0, sizeof(unsigned) * nn, S->stream));
+        // records never built read as empty (last = 0 prunes every entry); until the first
+        // rebuild marks the nodes, every record is built
+        YB_CUDA(cudaMemsetAsync(d.wide, 0, sizeof(WNode<R>) * nn, S->stream));
+        {
+            static const int kAll = 1;
+            YB_CUDA(cudaMemcpyAsync(d.wideAll, &kAll, sizeof(int), cudaMemcpyHostToDevice, S->stream));
+        }
         YB_CUDA(upload_layout());
         launch_bvh_reset(d, S->stream);
         YB_CUDA(cudaStreamSynchronize(S->stream));
@@ -706,7 +719,7 @@ struct Engine : EngineBase {
             if (rebuild) {
                 launch_bvh_rebuild(d, st, sortScratch, sortBytes, keyBits);
                 const int passes = d.nseg > 1 ? (keyBits + 7) / 8 : 0;
-                k += 3 + (d.nseg > 1 ? 2 + passes : 0) + 1 + 2;
+                k += 3 + (d.nseg > 1 ? 2 + passes : 0) + 1 + DEPTH_LAUNCHES + 2;
             } else {
                 launch_bvh_refit(d, st);
                 k += 2;
@@ -882,7 +895,7 @@ struct Engine : EngineBase {
                 mark(1);
                 launch_bvh_rebuild(d, st, sortScratch, sortBytes, keyBits);
                 const int passes = d.nseg > 1 ? (keyBits + 7) / 8 : 0;
-                launches[1] += 3 + (d.nseg > 1 ? 2 + passes : 0) + 1 + 2;
+                launches[1] += 3 + (d.nseg > 1 ? 2 + passes : 0) + 1 + DEPTH_LAUNCHES + 2;
             } else {
                 mark(2);
                 launch_bvh_refit(d, st);
@@ -966,10 +979,15 @@ struct Engine : EngineBase {
         uint64_t k = 0;
         if (mask & 1) { launch_init(d, st); k++; buf = 0; }
         if ((mask & 6) && d.nseg > 0) {
-            if (mask & 2) launch_bvh_rebuild(d, st, sortScratch, sortBytes, keyBits);
-            else launch_bvh_refit(d, st);
+            if (mask & 2) {
+                launch_bvh_rebuild(d, st, sortScratch, sortBytes, keyBits);
+                k += 3 + (d.nseg > 1 ? 2 + (keyBits + 7) / 8 : 0) + 1 + DEPTH_LAUNCHES + 2;
+            } else {
+                launch_bvh_refit(d, st);
+                k += 2;
+            }
             launch_traverse(d, st);
-            k += 3;
+            k += 2;
         }
         if (mask & 8) { launch_lists_step_limit(d, st); k++; }
         if (mask & 16) { launch_iter(d, buf, S->iterThreads, S->iterLanes, S->iterPipe, st); buf ^= 1; k++; }
