@@ -117,9 +117,50 @@ struct MetaData {
 };
 static_assert(sizeof(MetaData) == sizeof(yb_meta), "MetaData layout");
 
-struct Bounds {
+// The box type Sim::bounds() returns: the reference returns Kitten::LBVH::aabb, the 3-D
+// float Kitten::Bound (KittenEngine/includes/modules/Bound.h:7-72), whose members and methods
+// are restated here so code that grows, pads or tests the returned box compiles unchanged.
+struct aabb {
     vec3 min, max;
+    aabb() : min(fill(__builtin_huge_valf())), max(fill(-__builtin_huge_valf())) {}
+    explicit aabb(const vec3& c) : min(c), max(c) {}
+    aabb(const vec3& mn, const vec3& mx) : min(mn), max(mx) {}
+    vec3 center() const { return vec3((min[0] + max[0]) * 0.5f, (min[1] + max[1]) * 0.5f, (min[2] + max[2]) * 0.5f); }
+    void absorb(const aabb& b) {
+        for (int a = 0; a < 3; a++) {
+            min[a] = b.min[a] < min[a] ? b.min[a] : min[a];
+            max[a] = max[a] < b.max[a] ? b.max[a] : max[a];
+        }
+    }
+    void absorb(const vec3& p) { absorb(aabb(p)); }
+    bool contains(const vec3& p) const {
+        for (int a = 0; a < 3; a++)
+            if (!(min[a] <= p[a] && p[a] <= max[a])) return false;
+        return true;
+    }
+    bool contains(const aabb& b) const {
+        for (int a = 0; a < 3; a++)
+            if (!(min[a] <= b.min[a] && b.max[a] <= max[a])) return false;
+        return true;
+    }
+    bool intersects(const aabb& b) const {
+        for (int a = 0; a < 3; a++)
+            if (max[a] <= b.min[a] || min[a] >= b.max[a]) return false;
+        return true;
+    }
+    void pad(float p) { pad(vec3(p, p, p)); }
+    void pad(const vec3& p) {
+        for (int a = 0; a < 3; a++) {
+            min[a] -= p[a];
+            max[a] += p[a];
+        }
+    }
+    float volume() const { return (max[0] - min[0]) * (max[1] - min[1]) * (max[2] - min[2]); }
+
+   private:
+    static vec3 fill(float v) { return vec3(v, v, v); }
 };
+using Bounds = aabb;
 
 class Sim {
    public:
@@ -192,10 +233,10 @@ class Sim {
         return done;
     }
 
-    Bounds bounds() {
+    aabb bounds() {
         float b[6];
         check(yb_bounds(h_, -1, b));
-        return Bounds{vec3(b[0], b[1], b[2]), vec3(b[3], b[4], b[5])};
+        return aabb(vec3(b[0], b[1], b[2]), vec3(b[3], b[4], b[5]));
     }
 
     void printCollisionStats() {

@@ -114,7 +114,10 @@ yb_status yb_create(int32_t numVerts, yb_sim** out);
 
 /* Several scenes in one flat array (no reference counterpart; the batched form).
  * Scene s owns vertices [sum(vertsPerScene[0..s)), +vertsPerScene[s]).  precision is
- * YB_PRECISION_FP32 (production) or YB_PRECISION_FP64 (the FP64 build of the same kernels). */
+ * YB_PRECISION_FP32 (production) or YB_PRECISION_FP64 (the FP64 build of the same kernels).
+ * The scenes of a batch share one schedule: their yb_meta must agree on numItr,
+ * detectionPeriod and bvhRebuildPeriod, else configure, advance and gather return
+ * YB_ERR_INVALID_ARGUMENT (material and contact parameters may differ per scene). */
 yb_status yb_create_batch(int32_t numScenes, const int32_t* vertsPerScene, int32_t precision, yb_sim** out);
 
 /* Sim::~Sim, YarnBall.cu:53-85. */
@@ -146,11 +149,11 @@ yb_status yb_upload(yb_sim* sim);
 yb_status yb_download(yb_sim* sim);
 yb_status yb_zero_velocities(yb_sim* sim);
 
-/* Sim::advance(float h), step.cpp:101-120: ceil(dt/maxH) substeps, then the error check.
+/* Sim::advance(float h), step.cpp:36-55: ceil(dt/maxH) substeps, then the error check.
  * *advanced receives dt (the reference declares float but returns nothing). */
 yb_status yb_advance(yb_sim* sim, float dt, float* advanced);
 
-/* Sim::step(float), step.cpp:122-124: one advance(maxH). */
+/* Sim::step(float), step.cpp:57-59: one advance(maxH). */
 yb_status yb_step(yb_sim* sim, float dt);
 
 /* Sim::stepCount, YarnBall.h:163. */
@@ -370,11 +373,13 @@ yb_status yb_debug_sort_pairs(const uint64_t* keys, const int32_t* vals, int32_t
  * framework that owns the device-memory budget through its own pool, or a fixed-budget loop
  * in which an allocation (which can synchronise the device or fail under fragmentation) is
  * an error.  keysIn/valsIn/keysOut/valsOut are DEVICE pointers owned by the caller (inputs
- * are only read); stream is a cudaStream_t (NULL = legacy default).  Scratch is a fixed
+ * are only read; an output that overlaps its input gives YB_ERR_INVALID_ARGUMENT, so the
+ * sort is never in place); stream is a cudaStream_t (NULL = legacy default).  Scratch is a fixed
  * array compiled into the library (about 4.2 MB held on every GPU that loads it), so n is
  * limited to YB_SORT_NOALLOC_MAX_N; larger n returns YB_ERR_SCRATCH_TOO_SMALL.  No
  * cudaMalloc/cudaFree or allocating library call is made.  The first call on a device looks
- * the scratch address up (make it before any stream capture).  Calls share the scratch:
+ * the scratch address up (make it before any stream capture) and keeps it for the life of the
+ * process (do not reset the device while the library is in use).  Calls share the scratch:
  * calls that overlap on the GPU race and must be serialised.  Returns after the sort has
  * completed on `stream`. */
 #define YB_SORT_NOALLOC_MAX_N 262144

@@ -12,7 +12,7 @@
 //   recomputeStepLimitKernel   KittenEngine/YarnBall/sim/collision.cu:121-159
 //   cosseratItr                KittenEngine/YarnBall/sim/cosserat.cu:20-207
 //   quaternionLambdaItr        KittenEngine/YarnBall/sim/cosserat.cu:209-253
-//   Sim::advance               KittenEngine/YarnBall/sim/step.cpp:101-120
+//   Sim::advance               KittenEngine/YarnBall/sim/step.cpp:36-55
 //   segmentClosestPoints       KittenEngine/KittenEngine/includes/modules/Common.h:318-336
 //   Rotor ops                  KittenEngine/KittenEngine/includes/modules/Rotor.h:57-105,185-188
 //   hess3                      KittenEngine/KittenEngine/includes/modules/SymMat.h:8-107

@@ -70,7 +70,7 @@ void orc_set_state(orc_sim* s, const orc_vertex* verts, const float* vels, const
 void orc_set_meta(orc_sim* s, int scene, const orc_meta* meta);
 void orc_set_last_vel(orc_sim* s, const double* lastVel);
 void orc_set_schedule(orc_sim* s, uint64_t stepCounter);
-/* Sim::advance (step.cpp:101-120); returns 0 or 1 (contact overflow). */
+/* Sim::advance (step.cpp:36-55); returns 0 or 1 (contact overflow). */
 int orc_advance(orc_sim* s, float dt, float maxH);
 /* Phases: 1 predictor, 2 detection (+ step limit), 8 step limit, 16 one iteration, 32 advection.
  * h > 0 first sets lastH = h_old, h = h for every scene. */

@@ -4,6 +4,8 @@ import ctypes
 import os
 import re
 
+import pytest
+
 import oracle
 from yarnball_b200 import _abi
 
@@ -83,3 +85,23 @@ def test_scene_rng_is_xoshiro256ss_seeded_by_splitmix64():
         outs.append(r)
     lib = _abi.load()
     assert [lib.yb_rng_u64(0, i) for i in range(5)] == outs
+
+
+def test_batch_scenes_must_share_a_schedule():
+    """The scenes of a batch advance on one schedule (shared substep loop, detection cadence,
+    BVH rebuild clock and Newton launches), so configure refuses a batch whose scenes' meta
+    disagree on numItr, detectionPeriod or bvhRebuildPeriod (the reference keeps them per Sim,
+    YarnBall.h:63-114, step.cpp:46-49).  The check runs before any device work."""
+    import numpy as np
+
+    from yarnball_b200 import sim as ybsim
+
+    for field, value in [("numItr", 4), ("detectionPeriod", 2), ("bvhRebuildPeriod", 0.05)]:
+        s = ybsim.Sim(scenes=[8, 8])
+        for k in range(2):
+            s.verts["pos"][8 * k:8 * k + 8] = np.stack([np.arange(8) * 2e-3, np.full(8, 0.01 * k), np.zeros(8)], 1)
+        setattr(s.scene_meta(1), field, value)
+        with pytest.raises(RuntimeError):
+            s.configure()
+        assert s._lib.yb_configure(s._h, ctypes.c_float(1e-3)) == 1  # YB_ERR_INVALID_ARGUMENT
+        s.close()

@@ -10,10 +10,10 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def _build(tmp_path):
-    exe = str(tmp_path / "readme_example")
+def _build(tmp_path, name="readme_example"):
+    exe = str(tmp_path / name)
     cmd = ["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"),
-           os.path.join(ROOT, "tests", "cpp", "readme_example.cpp"),
+           os.path.join(ROOT, "tests", "cpp", name + ".cpp"),
            "-L", os.path.join(ROOT, "yarnball_b200", "_lib"), "-lyarnball_b200",
            "-Wl,-rpath," + os.path.join(ROOT, "yarnball_b200", "_lib"), "-o", exe]
     subprocess.run(cmd, check=True, capture_output=True)
@@ -22,6 +22,17 @@ def _build(tmp_path):
 
 def test_dropin_header_compiles_and_links(tmp_path):
     assert os.path.exists(_build(tmp_path))
+    assert os.path.exists(_build(tmp_path, "bounds_example"))
+
+
+@pytest.mark.gpu
+def test_dropin_bounds_is_a_box(tmp_path):
+    """bounds() returns a box with the reference's aabb methods (absorb, pad, contains,
+    intersects, center, volume) that holds every vertex after a frame."""
+    exe = _build(tmp_path, "bounds_example")
+    out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout.split()
+    assert out[0] == "64" and out[1] == "1" and out[2] == "1"
+    assert float(out[3]) > 0 and np.isfinite(float(out[4]))
 
 
 @pytest.mark.gpu

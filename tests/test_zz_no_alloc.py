@@ -18,7 +18,6 @@ import pytest
 import yarnball_b200 as yb
 from yarnball_b200 import _abi
 
-pytestmark = pytest.mark.gpu
 
 MAX_N = 262144  # YB_SORT_NOALLOC_MAX_N
 SCRATCH_TOO_SMALL = 13  # YB_ERR_SCRATCH_TOO_SMALL
@@ -38,22 +37,53 @@ def _noalloc_sort(keys, vals, bits):
     return st, kout.cpu().numpy().view(np.uint64), vout.cpu().numpy()
 
 
+def _stable_order(keys, bits):
+    """Reference order: a stable argsort on the low `bits` key bits (numpy, on the host)."""
+    mask = np.uint64((1 << bits) - 1) if bits < 64 else np.uint64(0xFFFFFFFFFFFFFFFF)
+    return np.argsort(keys & mask, kind="stable")
+
+
+@pytest.mark.gpu
 def test_noalloc_sort_matches_allocating_sort_twice():
     rng = np.random.default_rng(11)
-    cases = [(MAX_N, 39), (100003, 64)]  # two calls in a row, different sizes and key widths
+    # calls in a row with different sizes and key widths: a full 5-pass key at the size limit,
+    # an 8-pass key, a 1-pass key (odd pass count: the only pass writes the caller's output),
+    # a single pair, and bits = 0 (nothing to sort: a copy)
+    cases = [(MAX_N, 39), (100003, 64), (5000, 8), (1, 30), (777, 0)]
     for n, bits in cases:
-        keys = rng.integers(0, 2**min(bits, 63), size=n, dtype=np.uint64)
-        keys[: n // 4] = keys[1]  # duplicates exercise stability
+        # keys below 2**bits, as the BVH build passes them (bits = 0: any keys, left in place)
+        keys = rng.integers(0, 2**min(bits, 63) if bits else 2**63, size=n, dtype=np.uint64)
+        keys[: n // 4] = keys[n // 2]  # duplicates exercise stability
         vals = rng.permutation(n).astype(np.int32)
         st, ko, vo = _noalloc_sort(keys, vals, bits)
-        assert st == 0
+        assert st == 0, (n, bits)
+        order = _stable_order(keys, bits)
+        assert np.array_equal(ko, keys[order]), (n, bits)
+        assert np.array_equal(vo, vals[order]), (n, bits)
         rk, rv = yb.sort_pairs(keys, vals, bits)  # the existing (allocating) entry point
-        assert np.array_equal(ko, rk)
-        assert np.array_equal(vo, rv)
+        assert np.array_equal(ko, rk), (n, bits)
+        assert np.array_equal(vo, rv), (n, bits)
 
 
+@pytest.mark.gpu
 def test_noalloc_sort_rejects_sizes_above_its_scratch():
     keys = np.zeros(MAX_N + 1, np.uint64)
     vals = np.zeros(MAX_N + 1, np.int32)
     st, _, _ = _noalloc_sort(keys, vals, 30)
     assert st == SCRATCH_TOO_SMALL
+
+
+@pytest.mark.parametrize("alias", ["keys", "vals"])
+def test_noalloc_sort_refuses_output_overlapping_input(alias):
+    """An in-place call is refused before any device work: the argument check reads no
+    memory, so placeholder addresses are enough and this runs without a GPU."""
+    lib = _abi.load()
+    n = 1000
+    kin, vin, kout, vout = 0x100000, 0x200000, 0x300000, 0x400000
+    if alias == "keys":
+        kout = kin + 8 * 10  # overlaps the tail of the input keys
+    else:
+        vout = vin
+    st = lib.yb_sort_pairs_noalloc(ctypes.c_void_p(kin), ctypes.c_void_p(vin), ctypes.c_void_p(kout),
+                                   ctypes.c_void_p(vout), n, 30, None)
+    assert st == 1  # YB_ERR_INVALID_ARGUMENT

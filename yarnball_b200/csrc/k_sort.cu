@@ -201,8 +201,10 @@ int radix_sort_pairs(unsigned long long* keys[2], int* vals[2], int n, int bits,
 // array (about 4.2 MB) until the process exits.  The library looks its address up once per
 // device with cudaGetSymbolAddress (host code may not use the symbol itself as a device
 // address); that set-up happens inside the first call on each device, so make that first
-// call before any stream capture.  All calls share the array: calls whose GPU work overlaps
-// (two streams, or two host threads at once) race on it and must be serialised by the caller.
+// call before any stream capture.  The looked-up address is kept for the life of the process,
+// so the device may not be reset (cudaDeviceReset) while the library is in use.  All calls
+// share the array: calls whose GPU work overlaps (two streams, or two host threads at once)
+// race on it and must be serialised by the caller.
 namespace yb {
 namespace {
 
@@ -250,6 +252,14 @@ extern "C" yb_status yb_sort_pairs_noalloc(const uint64_t* keysIn, const int32_t
     if (n > NOALLOC_MAX_N) return YB_ERR_SCRATCH_TOO_SMALL;
     if (n == 0) return YB_OK;
     if (!keysIn || !valsIn || !keysOut || !valsOut) return YB_ERR_INVALID_ARGUMENT;
+    // The passes read the input while other blocks scatter into the output, so the output
+    // may not overlap the input (an in-place call would corrupt the keys).
+    auto overlap = [](const void* a, const void* b, size_t bytes) {
+        const uintptr_t x = (uintptr_t)a, y = (uintptr_t)b;
+        return x < y + bytes && y < x + bytes;
+    };
+    if (overlap(keysIn, keysOut, sizeof(uint64_t) * (size_t)n) || overlap(valsIn, valsOut, sizeof(int32_t) * (size_t)n))
+        return YB_ERR_INVALID_ARGUMENT;
     NoAllocScratch* S = nullptr;
     cudaError_t e = scratch_address(&S);
     if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? YB_ERR_OUT_OF_MEMORY : YB_ERR_CUDA;

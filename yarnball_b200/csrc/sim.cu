@@ -702,11 +702,8 @@ struct Engine : EngineBase {
         cudaMemcpyAsync(spDev, spHost, sizeof(SceneParams<R>) * S->numScenes, cudaMemcpyHostToDevice, S->stream);
     }
 
-    int num_itr() const {
-        int it = 0;
-        for (const auto& m : S->meta) it = std::max(it, (int)m.numItr);
-        return it;
-    }
+    // Newton iterations per substep: shared by every scene (validate_all_meta).
+    int num_itr() const { return (int)S->meta[0].numItr; }
 
     // Enqueues one substep on the stream; returns the number of kernels it launches.
     // One substep's kernels on S->stream; returns how many were launched.  With slots, the
@@ -1006,12 +1003,26 @@ yb_status engine_alloc(yb_sim* S) {
     return static_cast<Engine<float>*>(S->eng)->alloc();
 }
 
+// Every scene of a batch advances on one schedule: the substep loop, the detection cadence
+// and the BVH rebuild clock are shared, and every Newton launch covers all scenes.  The
+// reference keeps numItr, detectionPeriod and bvhRebuildPeriod per Sim (YarnBall.h:63-114,
+// step.cpp:46-49), so a batch whose scenes disagree on them is refused rather than run on
+// one scene's values.
+yb_status validate_schedule(const yb_sim* S) {
+    const yb_meta& m0 = S->meta[0];
+    for (const auto& m : S->meta)
+        if (m.numItr != m0.numItr || m.detectionPeriod != m0.detectionPeriod ||
+            !(m.bvhRebuildPeriod == m0.bvhRebuildPeriod))
+            return YB_ERR_INVALID_ARGUMENT;
+    return YB_OK;
+}
+
 yb_status validate_all_meta(yb_sim* S) {
     for (auto& m : S->meta) {
         const yb_status st = upload_meta_checks(m);
         if (st != YB_OK) return st;
     }
-    return YB_OK;
+    return validate_schedule(S);
 }
 
 }  // namespace
@@ -1148,6 +1159,10 @@ yb_status yb_configure(yb_sim* S, float density) {
         S->meta[s].maxSegLen = mx;
         S->meta[s].minSegLen = mn;
     }
+    {
+        const yb_status st = validate_schedule(S);
+        if (st != YB_OK) return st;
+    }
     if (S->eng) {  // re-configure: start from a fresh device state
         if (S->stream) cudaStreamSynchronize(S->stream);
         delete S->eng;
@@ -1224,7 +1239,7 @@ yb_status yb_advance(yb_sim* S, float dt, float* advanced) {
     if (advanced) *advanced = 0.f;
     if (!S->configured) return YB_ERR_NOT_CONFIGURED;
     if (!(dt > 0)) return YB_OK;
-    // step.cpp:101-120
+    // step.cpp:36-55
     const int steps = std::max(1, (int)std::ceil(dt / S->maxH));
     for (auto& m : S->meta) {
         m.lastH = m.h;
@@ -1765,7 +1780,7 @@ yb_status yb_debug_dx(yb_sim* S, double* dx4) {
 yb_status yb_step_residuals(yb_sim* S, double* maxDelta, int32_t capacity, int32_t* numIterations) {
     if (!S || !numIterations || capacity < 0 || (capacity > 0 && !maxDelta)) return YB_ERR_INVALID_ARGUMENT;
     if (!S->configured) return YB_ERR_NOT_CONFIGURED;
-    // one substep of maxH with the schedule of yb_advance (step.cpp:101-120)
+    // one substep of maxH with the schedule of yb_advance (step.cpp:36-55)
     const float dt = S->maxH;
     for (auto& m : S->meta) {
         m.lastH = m.h;
