@@ -356,6 +356,8 @@ yb_status yb_read_state_f64(yb_sim* sim, double* pos, double* vel, double* q);
  *   dx (4n in state precision widened to double).  NULL pointers are skipped. */
 yb_status yb_debug_contacts(yb_sim* sim, int32_t* numCols, int32_t* cols, float* stepLimit);
 yb_status yb_debug_dx(yb_sim* sim, double* dx4);
+/* Velocity of the previous substep (the predictor's lastVels, iteration.cu:19-20), 3n doubles. */
+yb_status yb_debug_last_vel(yb_sim* sim, double* lastVel3);
 
 /* Runs only the substep phases selected by mask on the current device state:
  * 1 = predictor (initItr), 2 = detection with BVH rebuild, 4 = detection with refit only,

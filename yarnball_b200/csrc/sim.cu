@@ -63,6 +63,7 @@ struct EngineBase {
     virtual yb_status load_device(FILE* f) = 0;
     virtual yb_status drive_pins(double dt) = 0;
     virtual yb_status residual_substep(int type, double* out, int cap, int* count) = 0;
+    virtual yb_status read_last_vel(double* out) = 0;
 };
 
 }  // namespace
@@ -813,6 +814,19 @@ struct Engine : EngineBase {
         if (e == cudaSuccess) e = cudaStreamSynchronize(S->stream);
         cudaFree(tmp);
         return cuda_status(e);
+    }
+
+    yb_status read_last_vel(double* out) override {
+        const size_t n = (size_t)S->n;
+        std::vector<V4<R>> h(n);
+        YB_CUDA(cudaMemcpyAsync(h.data(), d.lastVel, sizeof(V4<R>) * n, cudaMemcpyDeviceToHost, S->stream));
+        YB_CUDA(cudaStreamSynchronize(S->stream));
+        for (size_t i = 0; i < n; i++) {
+            out[3 * i] = (double)h[i].x;
+            out[3 * i + 1] = (double)h[i].y;
+            out[3 * i + 2] = (double)h[i].z;
+        }
+        return YB_OK;
     }
 
     yb_status contacts(int* numCols, int* cols, float* stepLimit) override {
@@ -1769,6 +1783,12 @@ yb_status yb_debug_contacts(yb_sim* S, int32_t* numCols, int32_t* cols, float* s
     if (!S) return YB_ERR_INVALID_ARGUMENT;
     if (!S->configured) return YB_ERR_NOT_CONFIGURED;
     return S->eng->contacts(numCols, cols, stepLimit);
+}
+
+yb_status yb_debug_last_vel(yb_sim* S, double* lastVel3) {
+    if (!S || !lastVel3) return YB_ERR_INVALID_ARGUMENT;
+    if (!S->configured) return YB_ERR_NOT_CONFIGURED;
+    return S->eng->read_last_vel(lastVel3);
 }
 
 yb_status yb_debug_dx(yb_sim* S, double* dx4) {

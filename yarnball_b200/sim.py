@@ -381,6 +381,11 @@ class Sim:
         check(self._lib.yb_debug_dx(self._h, ptr(dx, ctypes.c_double)), "dx")
         return dx[:, :3].copy()
 
+    def debug_last_vel(self):
+        lv = np.zeros((self.numVerts, 3))
+        check(self._lib.yb_debug_last_vel(self._h, ptr(lv, ctypes.c_double)), "lastVel")
+        return lv
+
     def debug_phases(self, mask, h=0.0):
         check(self._lib.yb_debug_phases(self._h, int(mask), float(h)), "phases")
 
