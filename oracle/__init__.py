@@ -2,8 +2,8 @@
 
 Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as the checker; never
 by the product.  The oracle is a C++/OpenMP restatement of the reference's substep
-(oracle/yb_oracle.cpp).  PARITY UNPINNED: the reference cannot be built or run here and has
-no golden vectors for this path; see yb_oracle.h.
+(oracle/yb_oracle.cpp).  It is pinned to the reference's own kernels, compiled unchanged from
+the reference's sources for the GPU by oracle/refbuild and run through oracle/reference.py.
 """
 import ctypes
 import os
@@ -40,6 +40,7 @@ _SIG = {
     "orc_penetrations": (ctypes.c_int64, [_v]),
     "orc_set_threads": (None, [ctypes.c_int]),
     "orc_max_threads": (ctypes.c_int, []),
+    "orc_math": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _f, _f, _f, _f, _f, _f]),
 }
 
 _LIB = None
@@ -47,6 +48,10 @@ _LIB = None
 
 def build():
     subprocess.run(["make", "-s", "-C", HERE], check=True)
+    # the reference's own kernels (oracle/_ref), when the reference's sources are present
+    from .refbuild import build as refbuild
+
+    refbuild.build()
 
 
 def load():
@@ -92,6 +97,34 @@ def set_kstretch(verts, k):
 
 def set_kbend(verts, qRests, k):
     load().orc_set_kbend(len(verts), verts.ctypes.data, _p(qRests, ctypes.c_float), k)
+
+
+_SCENES = None
+
+
+def random_walks_batch(seed, yarns_per_scene, yarn_lengths, seg_len=2e-3, cube=0.1, sigma=0.3, min_dist=None):
+    """The seeded batched random-walk geometry (yb_scene_random_walks_batch) from the host-only
+    build of the scene generator (no CUDA library loaded); same output as the engine's."""
+    global _SCENES
+    if _SCENES is None:
+        path = os.path.join(HERE, "_build", "libyb_scenes.so")
+        if not os.path.exists(path):
+            build()
+        lib = ctypes.CDLL(path)
+        lib.yb_scene_random_walks_batch.restype = ctypes.c_int
+        lib.yb_scene_random_walks_batch.argtypes = [ctypes.c_uint64, ctypes.c_int32, _i, _i, ctypes.c_float,
+                                                    ctypes.c_float, ctypes.c_float, ctypes.c_float, _f, ctypes.c_int32]
+        _SCENES = lib
+    if min_dist is None:  # 2 radius + 0.1 barrierThickness at yarn radius 0.5 mm
+        min_dist = float(2 * np.float32(0.05 * 0.5e-3) + 0.1 * np.float32(1.9 * 0.5e-3))
+    yps = np.ascontiguousarray(yarns_per_scene, dtype=np.int32)
+    lens = np.ascontiguousarray(yarn_lengths, dtype=np.int32)
+    out = np.zeros((int(lens.sum()), 3), np.float32)
+    st = _SCENES.yb_scene_random_walks_batch(int(seed), len(yps), _p(yps, ctypes.c_int32), _p(lens, ctypes.c_int32),
+                                             seg_len, cube, sigma, min_dist, _p(out, ctypes.c_float), 0)
+    if st != 0:
+        raise RuntimeError("batched random walk generation failed (%d)" % st)
+    return out
 
 
 def set_threads(t):

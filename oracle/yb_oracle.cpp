@@ -680,6 +680,69 @@ static inline rot<float> from_to(v3<float> from, v3<float> to) {
     return rot<float>{c.x, c.y, c.z, dot(from, h)};
 }
 
+// The oracle's FP32 math helpers over arrays, with the argument layout of the reference-kernel
+// harness (oracle/refbuild/ref_host.cpp, ref_math) so that tests can compare them bit for bit:
+// op 0 closest points (a0, a1, b0, b1 -> uv; relative to a0, as every kernel calls it),
+// 1 rotor product, 2 rotor rotation, 3 fromTo, 4 rotor normalisation, 5 hess3 outer-product
+// update and local solve.
+int orc_math(int op, int n, const float* a, const float* b, const float* c, const float* d, float* out, float* out2) {
+    for (int i = 0; i < n; i++) {
+        switch (op) {
+            case 0: {
+                const float* p = a + 12 * (size_t)i;
+                const v3<float> a0 = mk(p[0], p[1], p[2]);
+                float u, v;
+                closest(mk(p[3], p[4], p[5]) - a0, mk(p[6], p[7], p[8]) - a0, mk(p[9], p[10], p[11]) - a0, false, u, v);
+                out[2 * i] = u;
+                out[2 * i + 1] = v;
+                break;
+            }
+            case 1: {
+                const float* l = a + 4 * (size_t)i;
+                const float* r = b + 4 * (size_t)i;
+                const rot<float> q = rmul(rot<float>{l[0], l[1], l[2], l[3]}, rot<float>{r[0], r[1], r[2], r[3]});
+                out[4 * i] = q.x; out[4 * i + 1] = q.y; out[4 * i + 2] = q.z; out[4 * i + 3] = q.w;
+                break;
+            }
+            case 2: {
+                const float* q = a + 4 * (size_t)i;
+                const float* v = b + 3 * (size_t)i;
+                const v3<float> r = rrotate(rot<float>{q[0], q[1], q[2], q[3]}, mk(v[0], v[1], v[2]));
+                out[3 * i] = r.x; out[3 * i + 1] = r.y; out[3 * i + 2] = r.z;
+                break;
+            }
+            case 3: {
+                const float* f = a + 3 * (size_t)i;
+                const float* t = b + 3 * (size_t)i;
+                const rot<float> q = from_to(mk(f[0], f[1], f[2]), mk(t[0], t[1], t[2]));
+                out[4 * i] = q.x; out[4 * i + 1] = q.y; out[4 * i + 2] = q.z; out[4 * i + 3] = q.w;
+                break;
+            }
+            case 4: {
+                const float* v = a + 4 * (size_t)i;
+                const rot<float> r{v[0], v[1], v[2], v[3]};
+                const rot<float> q = rscale(1.0f / rlen(r), r);
+                out[4 * i] = q.x; out[4 * i + 1] = q.y; out[4 * i + 2] = q.z; out[4 * i + 3] = q.w;
+                break;
+            }
+            case 5: {
+                hs3<float> H;
+                for (int k = 0; k < 6; k++) H.d[k] = a[6 * (size_t)i + k];
+                const float* nn = b + 3 * (size_t)i;
+                houter(H, mk(nn[0], nn[1], nn[2]), c[i]);
+                for (int k = 0; k < 6; k++) out[6 * (size_t)i + k] = H.d[k];
+                const float* f = d + 3 * (size_t)i;
+                const v3<float> x = hsolve(H, mk(f[0], f[1], f[2]));
+                out2[3 * i] = x.x; out2[3 * i + 1] = x.y; out2[3 * i + 2] = x.z;
+                break;
+            }
+            default:
+                return -2;
+        }
+    }
+    return 0;
+}
+
 int orc_configure(int n, float density, orc_vertex* verts, float* qs, float* qRests, float* initialInvMasses,
                   float* maxSegLen, float* minSegLen) {
     float mx = 0, mn = FLT_MAX;

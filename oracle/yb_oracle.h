@@ -6,11 +6,12 @@
  * algorithm (YarnBall::Sim::advance and the kernels it launches), written independently of
  * the CUDA engine, evaluated in FP64 (the accuracy oracle) or FP32 (the CPU baseline).
  *
- * PARITY UNPINNED: the reference cannot be built or run here (it needs glm, jsoncpp and an
- * LBVH submodule that are absent, and an MSBuild toolchain) and ships no tests, golden
- * vectors or fixtures for this path.  The restatement is checked instead against
- * independent derivations (finite differences, brute-force minimisation, FP64 LU solves,
- * geometric invariants) and against a second, pure-numpy restatement in the tests.
+ * Pinned to the reference: oracle/refbuild compiles the reference's own kernels and math
+ * headers unchanged for the GPU (against a restatement of the absent glm and a stand-in for
+ * the absent LBVH), and the GPU tests compare them with this restatement (tests/
+ * test_gpu_reference.py).  It is also checked against independent derivations (finite
+ * differences, brute-force minimisation, FP64 LU solves, geometric invariants) and against a
+ * second, pure-numpy restatement in the CPU tests.
  *
  * Semantic choices (the reference's own kernels are scheduling dependent):
  *   - strict Jacobi: iteration k reads only iteration k-1's dx and orientations;
@@ -60,6 +61,9 @@ int orc_configure(int n, float density, orc_vertex* verts, float* qs, float* qRe
 void orc_set_kstretch(int n, orc_vertex* verts, float k);
 void orc_set_kbend(int n, const orc_vertex* verts, float* qRests, float k);
 int orc_upload_meta(orc_meta* m); /* derives the detection radii; 0 or an error code */
+/* The FP32 math helpers over n inputs (op 0 closest points, 1 rotor product, 2 rotation,
+ * 3 fromTo, 4 rotor normalisation, 5 hess3 update + solve); see yb_oracle.cpp. */
+int orc_math(int op, int n, const float* a, const float* b, const float* c, const float* d, float* out, float* out2);
 
 typedef struct orc_sim orc_sim;
 orc_sim* orc_create(int n, int mode);

@@ -3,6 +3,7 @@ second restatement in tests/np_ref.py.  PARITY UNPINNED: the reference itself ca
 here and ships no golden vectors, so these checks pin the oracle to mathematics and to an
 independent implementation instead."""
 import ctypes
+import os
 
 import numpy as np
 import pytest
@@ -190,3 +191,29 @@ def test_engine_host_configure_is_bit_exact_with_oracle():
     assert np.array_equal(v.view(np.uint8), s.verts.copy().view(np.uint8))
     assert np.array_equal(q, s.qs) and np.array_equal(qr, s.qRests)
     assert np.array_equal(im, s.initialInvMasses)
+
+
+def test_reference_kernel_build():
+    """The recipe in oracle/refbuild compiles the reference's own kernels from its sources
+    (when they are present here) into oracle/_ref, and the host harness loads and exports its
+    entry points without a GPU."""
+    from oracle import reference as R
+    from oracle.refbuild import build as rb
+
+    if os.path.isdir(os.path.join(rb.reference_root(), "KittenEngine", "YarnBall")):
+        assert rb.build()
+    if not R.available():
+        pytest.skip("reference sources absent and no prebuilt oracle/_ref")
+    lib = ctypes.CDLL(R.LIB_PATH)
+    for name in R._SIG:
+        assert hasattr(lib, name), name
+    for p in R.FATBINS.values():
+        assert os.path.getsize(p) > 10000
+
+
+def test_oracle_scene_generator_matches_engine_generator():
+    """The host-only build of the scene generator that the CPU reference arm uses gives the
+    engine library's geometry, bit for bit."""
+    spec = scenes.batched_spec(7, 3, 10**6)
+    flat = np.concatenate(spec[1]).astype(np.int32)
+    assert np.array_equal(oracle.random_walks_batch(7, spec[0], flat), scenes.random_walks_batch(7, spec[0], flat))
