@@ -11,8 +11,9 @@ each yarn pinned.  Synthetic, seeded (no dataset exists for this path).
   python bench.py [--gpus N --steps K --warmup W]      # the CUDA engine (one JSON line)
   python bench.py --impl reference ...                 # the reference algorithm on the host
 
-Under torchrun every rank simulates its own batch (seed offset by rank): weak scaling, no
-collective on the data path; the time is the max over ranks of the device time.
+Under torchrun the scenes of the one batch are split over the ranks by greedy bin packing of
+their vertex counts (strong scaling, no collective on the data path); the time is the max over
+ranks of the device time.
 """
 import argparse
 import json
@@ -52,8 +53,9 @@ def parse():
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     p.add_argument("--cap", type=int, default=8388608, help="vertex cap of the batched workload")
     p.add_argument("--shape", default="", help="fixed Newton kernel shape threads,lanes,pipelined (default: autotune)")
-    p.add_argument("--workload", default="batched", choices=["batched", "serve", "twist", "pile"])
+    p.add_argument("--workload", default="batched", choices=["batched", "serve", "twist", "pile", "readme"])
     p.add_argument("--pile-frames", type=int, default=60, help="pile: frames")
+    p.add_argument("--readme-frames", type=int, default=150, help="readme: frames")
     p.add_argument("--rate", type=float, default=4.0, help="serve: Poisson arrival rate (requests/s)")
     p.add_argument("--duration", type=float, default=10.0, help="serve: arrival window (s)")
     p.add_argument("--frames", type=int, default=30, help="serve: frames per request; twist: frames (0 = 300)")
@@ -76,7 +78,7 @@ def workload_desc(spec):
         "step": "advance(1/30 s) of the whole batch (%d substeps of h=1/%d s)" % (SUBSTEPS, SUBSTEPS * 30),
         "l2": "inputs larger than L2 (state ~0.8 KB/vertex x %.1fM vertices), no flush" % (n / 1e6),
         "seed": SEED,
-        "parallelism": "one independent batch per GPU (weak scaling)",
+        "parallelism": "one GPU",
     }
 
 
@@ -163,8 +165,10 @@ def oracle_sample(spec, target_verts, mode, seed=SEED):
     while k < len(yarns) and tot < target_verts:
         tot += int(lens[k].sum())
         k += 1
-    flat = np.concatenate(lens).astype(np.int32)
-    pos_all = scenes.random_walks_batch(seed, yarns, flat)
+    # the same seeded geometry as the GPU batch, from the host-only build of the generator
+    # (this CPU path loads no CUDA library); scene s depends only on (seed, s)
+    flat = np.concatenate(lens[:k]).astype(np.int32)
+    pos_all = oracle.random_walks_batch(seed, yarns[:k], flat)
     counts = [int(l.sum()) for l in lens[:k]]
     offs = np.concatenate([[0], np.cumsum(counts)])
     pos_list = [pos_all[offs[s]:offs[s + 1]] for s in range(k)]
@@ -193,9 +197,10 @@ def cpu_baseline_sample(spec, target_verts=1_000_000, reps_seconds=10.0, mode=No
 
 
 def run_reference(args):
-    """Reference arm: the reference's algorithm as restated by the CPU oracle (the reference
-    itself does not build here), FP32, all host threads; each step = one substep of a bounded
-    sample of the batch."""
+    """Reference arm: the reference's algorithm on the host cores (the reference has no CPU path
+    for it, so this is the CPU oracle's restatement, pinned to the reference's kernels by the
+    tests), FP32, all host threads; each step = one substep of a bounded sample of the batch.
+    Loads no CUDA library."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -203,8 +208,13 @@ def run_reference(args):
     from yarnball_b200 import scenes
 
     spec = scenes.batched_spec(SEED, 512, args.cap)
-    n, cfg = workload_desc(spec)
+    _, cfg = workload_desc(spec)
     orc, k, tot = oracle_sample(spec, 400_000, oracle.FP32)
+    # the workload is the GPU arm's; each timed step is a bounded sample of it
+    cfg["timed_sample"] = {
+        "scenes": k, "vertices": tot, "yarns": int(sum(spec[0][:k])), "substeps_per_step": 1,
+        "what": "the first %d scenes (%d vertices) of this workload, one substep of h=1/%d s per step "
+                "(the metric is per vertex-substep, as the GPU arm's)" % (k, tot, SUBSTEPS * 30)}
     h = float(np.float32(FRAME) / np.float32(SUBSTEPS))
     for _ in range(args.warmup):
         orc.advance(h, h)
@@ -218,12 +228,13 @@ def run_reference(args):
     out = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": cfg,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "the reference (CUDA/MSBuild, needs glm, jsoncpp and an absent LBVH submodule) does not build "
-                "offline; its substep is run as the CPU restatement in oracle/ (strict Jacobi, FP32, OpenMP)",
+        "note": "the reference has no CPU implementation of the substep; this arm runs the oracle's CPU "
+                "restatement of it (oracle/, strict Jacobi, FP32, OpenMP), which the tests pin to the "
+                "reference's own kernels (compiled unchanged from its sources for the GPU by oracle/refbuild)",
     }
     print(json.dumps(out))
 
@@ -244,9 +255,18 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     from yarnball_b200 import scenes, sharding
 
-    spec = scenes.batched_spec(SEED + 1000 * rank, 512, args.cap)
-    n, cfg = workload_desc(spec)
-    sim, _ = scenes.build_batched(seed=SEED + 1000 * rank, spec=spec)
+    # One batch for the whole job: its scenes are split over the ranks by greedy bin packing of
+    # their vertex counts (no collective on the data path; strong scaling).
+    spec = scenes.batched_spec(SEED, 512, args.cap)
+    _, cfg = workload_desc(spec)
+    sizes = [int(l.sum()) for l in spec[1]]
+    parts = sharding.partition_scenes(sizes, world)
+    mine = parts[rank]
+    n = int(sum(sizes[i] for i in mine))
+    if world > 1:
+        cfg["parallelism"] = "scenes split over %d GPUs by greedy bin packing (strong scaling)" % world
+        cfg["vertices_per_rank_max"] = int(max(sum(sizes[i] for i in p) for p in parts))
+    sim, _ = scenes.build_batched(seed=SEED, spec=spec, indices=mine)
     stream = torch.cuda.Stream()
     sim.set_stream(stream.cuda_stream)
     for _ in range(args.warmup):
@@ -358,7 +378,7 @@ def run_ours(args):
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches) * world,
             "clocks": ck, "plain": plain,
             "batched_over_plain": (value / plain["value"]) if plain else None,
@@ -677,6 +697,116 @@ def run_pile(args):
     print(json.dumps(out))
 
 
+def run_readme(args):
+    """Config 1, the README two-yarn scene (README.md:104-127; 64 vertices): 150 frames of
+    advance(1/30 s) = 5100 substeps through the plain drop-in path, device-timed; beside it the
+    same frames on the reference's own kernels on this GPU (compiled unchanged from its sources
+    by oracle/refbuild, when built; their BVH query is a brute-force stand-in, trivial at 64
+    vertices) and on the CPU oracle (FP32, OpenMP).  Accuracy: the engine's positions against
+    the FP64 oracle after the first and the last frame (relative to the motion), and the largest
+    distance between the engine's and the reference kernels' trajectories over the run."""
+    import torch
+
+    import oracle
+    from yarnball_b200 import scenes
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    frames = max(1, args.readme_frames)
+    sim = scenes.build_readme()
+    sim.download()
+    v, vel, q, qr = sim.verts.copy(), sim.vels.astype(np.float32).copy(), sim.qs.copy(), sim.qRests.copy()
+    meta = sim.scene_meta(0).as_struct()
+    x0 = v["pos"].astype(np.float64)
+    stream = torch.cuda.Stream()
+    sim.set_stream(stream.cuda_stream)
+    for _ in range(max(0, args.warmup)):  # warm-up on separate copies: the timed run starts at t = 0
+        w = scenes.build_readme()
+        w.advance(FRAME)
+        w.close()
+    torch.cuda.synchronize()
+    l0 = sim.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(frames):
+        sim.advance(FRAME)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = sim.launch_count() - l0
+    work = 64 * SUBSTEPS * frames
+    final = sim.read_state_f64()[0]
+    sim.close()
+    # end to end with host copies every frame (upload, advance, download)
+    sim = scenes.build_readme()
+    w0 = time.perf_counter()
+    for _ in range(frames):
+        sim.upload()
+        sim.advance(FRAME)
+        sim.download()
+    wall_e2e = time.perf_counter() - w0
+    sim.close()
+    # accuracy against the FP64 oracle, distance to the reference kernels' trajectory
+    eng = scenes.build_readme()
+    orc = oracle.from_sim(eng, mode=oracle.FP64)
+    refk, ref_err = None, None
+    try:
+        from oracle import reference as R
+
+        if R.available():
+            refk = R.RefSim(v, vel, q, qr, meta, variant="fma")
+        else:
+            ref_err = "reference kernels not built (oracle/_ref)"
+    except Exception as e:  # reported, not fatal: the reference build is test infrastructure
+        ref_err = str(e)
+    acc, traj = {}, 0.0
+    for f in range(1, frames + 1):
+        eng.advance(FRAME)
+        orc.advance(FRAME, MAX_H)
+        pe = eng.read_state_f64()[0]
+        if refk is not None:
+            refk.advance(FRAME)
+            traj = max(traj, float(np.abs(pe - refk.read("verts")["pos"].astype(np.float64)).max()))
+        if f in (1, frames):
+            po = orc.state()["pos"]
+            acc["frame_%d" % f] = float(np.abs(pe - po).max() / max(np.abs(po - x0).max(), 1e-30))
+    eng.close()
+    orc.close()
+    if refk is not None:
+        refk.close()
+        timer = R.RefSim(v, vel, q, qr, meta, variant="fma")
+        timer.advance(FRAME)  # warm-up (module load)
+        timer.close()
+        timer = R.RefSim(v, vel, q, qr, meta, variant="fma")
+        rc, rms = timer.time_advance(FRAME, frames)
+        timer.close()
+        ref_cuda = {"value": work / (rms / 1e3), "unit": UNIT, "ms": rms, "status": rc,
+                    "what": "the reference's own kernels (fused multiply-adds, as its build compiles them) on "
+                            "this GPU, launched with the reference's shapes and schedule; brute-force BVH stand-in"}
+    else:
+        ref_cuda = {"unavailable": ref_err}
+    orc = oracle.from_sim(scenes.build_readme(), mode=oracle.FP32)
+    t0 = time.perf_counter()
+    for _ in range(frames):
+        orc.advance(FRAME, MAX_H)
+    cpu_s = time.perf_counter() - t0
+    orc.close()
+    out = {"metric": "vertex-substeps/s (README two-yarn scene, plain advance)", "value": work / (ms / 1e3),
+           "unit": UNIT, "frames": frames, "substeps": SUBSTEPS * frames, "ms": ms, "ms_per_frame": ms / frames,
+           "gpu_launches": int(launches),
+           "e2e": {"value": work / wall_e2e, "unit": UNIT, "wall_s": wall_e2e,
+                   "h2d_bytes_per_step": 64 * (32 + 12 + 16 + 16), "d2h_bytes_per_step": 64 * (32 + 12 + 16),
+                   "api": "yb_upload + yb_advance + yb_download per frame (host wall clock)"},
+           "reference_cuda": ref_cuda,
+           "cpu_baseline": {"value": work / cpu_s, "unit": UNIT, "cores": oracle.max_threads(), "kind": "port",
+                            "sample": "the same %d frames, FP32 OpenMP" % frames},
+           "accuracy": {"rel_err_vs_fp64_oracle": acc, "bound": 1e-4,
+                        "max_dist_to_reference_kernels_m": traj if refk is not None else None,
+                        "final_displacement_m": float(np.abs(final - x0).max())},
+           "config": {"workload": "README two-yarn scene: 2 yarns x 32 vertices, pins 0/32/63, kCollision 1e-7, "
+                                  "kBend 1e-8, kStretch 2e-2, maxH 1e-3, advance(1/30) x %d" % frames}}
+    print(json.dumps(out))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -687,6 +817,8 @@ def main():
         run_twist(args)
     elif args.workload == "pile":
         run_pile(args)
+    elif args.workload == "readme":
+        run_readme(args)
     else:
         run_ours(args)
 

@@ -66,3 +66,19 @@ def test_two_gloo_ranks_agree_on_partition_and_reduce():
         assert stats[0] == 2.0 and stats[1] == float(sum(sizes))
     assert sorted(res[0][0] + res[1][0]) == list(range(len(sizes)))
     np.testing.assert_equal(len(set(res[0][0]) & set(res[1][0])), 0)
+
+
+def test_rank_subsets_hold_the_one_gpu_geometry():
+    """Each rank of a multi-GPU run builds its scenes of the one batch: their geometry equals
+    those scenes' slices of the 1-GPU batch, and the ranks together hold every scene once."""
+    spec = scenes.batched_spec(seed=7, num_scenes=30, cap=600_000)
+    full = scenes.batched_positions(7, spec)
+    sizes = [int(l.sum()) for l in spec[1]]
+    parts = sharding.partition_scenes(sizes, 4)
+    seen = []
+    for p in parts:
+        sub = scenes.batched_positions(7, spec, p)
+        for i, pos in zip(p, sub):
+            assert np.array_equal(pos, full[i])
+        seen += p
+    assert sorted(seen) == list(range(len(sizes)))

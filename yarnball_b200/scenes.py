@@ -216,15 +216,37 @@ def batched_spec(seed=7, num_scenes=512, cap=8388608, max_yarns=64, min_len=64, 
     return yarns, lens, kbend
 
 
-def build_batched(seed=7, num_scenes=512, cap=8388608, precision="fp32", spec=None, threads=0):
-    yarns, lens, kbend = spec if spec is not None else batched_spec(seed, num_scenes, cap)
-    flat = np.concatenate(lens).astype(np.int32)
-    pos = random_walks_batch(seed, yarns, flat, threads=threads)
+def batched_positions(seed, spec, indices=None, threads=0):
+    """Vertex positions of the scenes `indices` (default: all) of a batched spec, one array per
+    scene.  Scene i is seeded from (seed, i), its index in the full spec, so a subset (the
+    scenes one rank of a multi-GPU run simulates) holds exactly the geometry those scenes have
+    in the whole batch."""
+    yarns, lens, _ = spec
+    if indices is None:
+        indices = list(range(len(yarns)))
+    last = max(indices) + 1 if len(indices) else 0
+    if last == 0:
+        return []
+    flat = np.concatenate(lens[:last]).astype(np.int32)
+    pos = random_walks_batch(seed, yarns[:last], flat, threads=threads)
+    offs = np.concatenate([[0], np.cumsum([int(l.sum()) for l in lens[:last]])]).astype(np.int64)
+    return [pos[offs[i]:offs[i + 1]] for i in indices]
+
+
+def build_batched(seed=7, num_scenes=512, cap=8388608, precision="fp32", spec=None, threads=0, indices=None):
+    """The batched workload (or the subset `indices` of its scenes) as one batch."""
+    full = spec if spec is not None else batched_spec(seed, num_scenes, cap)
+    if indices is None:
+        indices = list(range(len(full[0])))
+    yarns = [full[0][i] for i in indices]
+    lens = [full[1][i] for i in indices]
+    kbend = [full[2][i] for i in indices]
+    pos_list = batched_positions(seed, full, indices, threads=threads)
     counts = [int(l.sum()) for l in lens]
     sim = Sim(scenes=counts, precision=precision)
     off = 0
     for s, l in enumerate(lens):
-        fill_yarns(sim, pos[off:off + counts[s]], l, offset=off, pin_first=True)
+        fill_yarns(sim, pos_list[s], l, offset=off, pin_first=True)
         off += counts[s]
     sim.set_meta_all(**PILE_META)
     sim.configure()
