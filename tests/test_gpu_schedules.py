@@ -124,7 +124,7 @@ def test_schedule_variant_vs_fp64_oracle(name):
 
 
 def _dense_batch(precision, num_scenes=24, seed=21):
-    """A batch of small, dense pile scenes (3 cm cubes) of uneven size: contact-heavy."""
+    """A batch of small, dense pile scenes (2.2 cm cubes) of uneven size: contact-heavy."""
     rng = np.random.default_rng(seed)
     yarns = rng.integers(6, 24, size=num_scenes)
     verts = rng.integers(40, 96, size=num_scenes)
@@ -133,7 +133,7 @@ def _dense_batch(precision, num_scenes=24, seed=21):
     off = 0
     for s in range(num_scenes):
         lens = np.full(int(yarns[s]), int(verts[s]), np.int32)
-        pos = scenes.random_walks(seed * 1000 + s, lens, cube=0.03)
+        pos = scenes.random_walks(seed * 1000 + s, lens, cube=0.022)
         scenes.fill_yarns(sim, pos, lens, offset=off)
         off += counts[s]
     sim.set_meta_all(**scenes.PILE_META)
