@@ -197,6 +197,11 @@ yb_status yb_get_tuning(yb_sim* sim, int32_t* iterThreads, int32_t* lanesPerVert
 yb_status yb_autotune(yb_sim* sim, int32_t* bestThreads, int32_t* bestLanes, int32_t* bestPipelined,
                       float* bestMs);
 
+/* Broadphase walk of the BVH: packet = 1 (default) walks the tree once per warp for 32
+ * consecutive queries, packet = 0 once per query.  The contact lists are identical. */
+yb_status yb_set_traversal(yb_sim* sim, int32_t packet);
+yb_status yb_get_traversal(yb_sim* sim, int32_t* packet);
+
 /* Launch the simulation's work on `stream` (a cudaStream_t; NULL returns to the simulation's
  * own stream).  Lets a caller order the engine with its own work and time it with events. */
 yb_status yb_set_stream(yb_sim* sim, void* stream);

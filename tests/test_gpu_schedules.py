@@ -255,3 +255,29 @@ def test_diagnostics_vs_oracle_fp64_evaluation():
         assert abs(g[key] - o[key]) <= 1e-9 * max(abs(o[key]), 1e-30), (key, g[key], o[key])
     assert g["kinetic"] > 0 and g["barrier"] > 0 and g["pairs"] > 0
     sim.close()
+
+
+@pytest.mark.parametrize("which", ["pile", "batch"])
+def test_packet_and_per_query_traversal_give_the_same_lists(which):
+    """The broadphase walk per warp of 32 queries (the default) and per query keep the same
+    pairs, on a rebuilt and on a refitted tree; both equal the oracle's."""
+    if which == "pile":
+        build = lambda: scenes.build_pile(seed=1)  # noqa: E731  (the full 262,144-vertex pile)
+    else:
+        spec = scenes.batched_spec(seed=7, num_scenes=24, cap=1500000)
+        build = lambda: scenes.build_batched(seed=7, spec=spec)[0]  # noqa: E731
+    out = {}
+    for packet in (True, False):
+        sim = build()
+        sim.set_traversal(packet)
+        sim.advance(FRAME)
+        orc = _oracle_from(sim, oracle.FP32_MIXED)
+        sim.debug_phases(1 | 4, H)  # refitted tree
+        orc.phases(1 | 2, H)
+        _compare_lists(sim, orc)
+        sim.debug_phases(2)         # rebuilt tree on the same state
+        out[packet] = sim.debug_contacts()
+        _compare_lists(sim, orc)
+        sim.close()
+        orc.close()
+    assert np.array_equal(out[True][0], out[False][0])

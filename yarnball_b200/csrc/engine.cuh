@@ -168,6 +168,7 @@ struct Dev {
     int* sceneLast;   // sorted position of the last leaf of each scene's subtree
     unsigned* travNext;   // next query (sorted position) handed out by the traversal
     int travBlocks;       // persistent traversal grid
+    int travPacket;       // 1: one walk per warp for 32 queries (k_traverse_packet), 0: one per lane
     unsigned long long* keys[2];
     int* vals[2];
     unsigned* sceneBox;   // 6 ordered-uint per scene: min xyz, max xyz of segment midpoints

@@ -661,6 +661,139 @@ __global__ void __launch_bounds__(128) k_lists(Dev<R> d, int sortLists) {
     if (valid) d.stepLim[k] = d.sp[sc].useStepLimit ? m : yinf<R>();
 }
 
+// Packet traversal: a warp walks the tree once for 32 consecutive queries (consecutive sorted
+// positions, so neighbouring segments in Morton order).  Every lane tests its own box against
+// the entries of the node the warp has loaded (one record, read by all lanes at the same
+// address); the warp descends into an internal entry when any of its lanes overlaps it, keeping
+// one stack per warp in shared memory.  The walk is the union of the 32 walks of k_traverse,
+// but each node is loaded once per warp instead of once per lane, so the chain of dependent
+// node loads is paid once per 32 queries.  Each lane keeps exactly the leaves k_traverse keeps
+// for it (its own box, leaves after its sorted position), so the pair set is identical; lanes
+// of different scenes in one warp walk their scenes one after the other.
+constexpr int PK_STACK = 64;
+
+template <typename R>
+__global__ void __launch_bounds__(TRAV_THREADS) k_traverse_packet(Dev<R> d) {
+    __shared__ int sQx[TRAV_WARPS][TRAV_QCAP];
+    __shared__ int sQy[TRAV_WARPS][TRAV_QCAP];
+    __shared__ int sStack[TRAV_WARPS][PK_STACK];
+    const unsigned FULL = 0xffffffffu;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nseg = d.nseg;
+    int* stack = sStack[warp];
+    int qn = 0;  // queued candidates (identical in every lane)
+    auto drain = [&](bool all) {
+        while (qn >= 32 || (all && qn > 0)) {
+            const int m = min(qn, 32);
+            if (lane < m) {
+                const int x = sQx[warp][qn - m + lane];
+                const int y = sQy[warp][qn - m + lane];
+                if (pair_keep(d, x, y, d.sp[scene_of(d.vp[x].flags)])) {
+                    list_append(d, x, y);
+                    list_append(d, y, x);
+                }
+            }
+            qn -= m;
+            __syncwarp();
+        }
+    };
+    while (true) {
+        int base = 0;
+        if (lane == 0) base = (int)atomicAdd(d.travNext, 32u);
+        base = __shfl_sync(FULL, base, 0);
+        if (base >= nseg) break;
+        const int qi = base + lane;
+        bool live = qi < nseg;
+        int k = -1, sc = -1;
+        Box<R> qb;
+        if (live) {
+            QRec<R> r;
+            if constexpr (sizeof(R) == 4) {
+                const float4* src = reinterpret_cast<const float4*>(d.qrec + qi);
+                float4* dst = reinterpret_cast<float4*>(&r);
+                dst[0] = __ldg(src);
+                dst[1] = __ldg(src + 1);
+            } else {
+                r = d.qrec[qi];
+            }
+            k = r.k;
+            sc = r.sc;
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                qb.mn[a] = r.mn[a];
+                qb.mx[a] = r.mx[a];
+            }
+            live = d.sceneRoot[sc] >= 0 && d.sceneLast[sc] > qi;  // a leaf root has no pairs
+        }
+        unsigned todo = __ballot_sync(FULL, live);
+        while (todo) {
+            const int leader = __ffs(todo) - 1;
+            const int wsc = __shfl_sync(FULL, sc, leader);
+            const bool mine = live && sc == wsc;
+            todo &= ~__ballot_sync(FULL, mine);
+            int node = d.sceneRoot[wsc];
+            int top = 0, steps = 0;
+            while (node >= 0) {
+                if (node >= nseg - 1 || ++steps > nseg) {  // only a corrupt tree gets here
+                    if (lane == 0) atomicOr(&d.err[EW_INTERNAL], IE_BVH_STACK);
+                    break;
+                }
+                WNode<R> w;
+                trav_load_wide(d.wide, node, w);
+                int cand[4];
+                int nc = 0;
+                int next = -1;
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    const bool hit = mine && w.last[e] > qi && qb.mn[0] <= w.mx[0][e] && w.mn[0][e] <= qb.mx[0] &&
+                                     qb.mn[1] <= w.mx[1][e] && w.mn[1][e] <= qb.mx[1] && qb.mn[2] <= w.mx[2][e] &&
+                                     w.mn[2][e] <= qb.mx[2];
+                    const int c = w.code[e];  // the same in every lane
+                    if (c < 0) {
+                        if (hit) cand[nc++] = -c - 1;
+                    } else if (__any_sync(FULL, hit)) {
+                        if (next < 0) {
+                            next = c;
+                        } else if (top < PK_STACK) {
+                            if (lane == 0) stack[top] = c;
+                            top++;
+                        } else if (lane == 0) {
+                            atomicOr(&d.err[EW_INTERNAL], IE_BVH_STACK);
+                        }
+                    }
+                }
+                // queue this lane's candidates at its offset (warp scan of the counts)
+                int incl = nc;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(FULL, incl, o);
+                    if (lane >= o) incl += y;
+                }
+                const int at = qn + incl - nc;
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    if (e < nc) {
+                        sQx[warp][at + e] = min(k, cand[e]);
+                        sQy[warp][at + e] = max(k, cand[e]);
+                    }
+                }
+                qn += __shfl_sync(FULL, incl, 31);
+                __syncwarp();
+                drain(false);
+                if (next >= 0) {
+                    node = next;
+                } else if (top > 0) {
+                    node = stack[--top];
+                } else {
+                    node = -1;
+                }
+            }
+            __syncwarp();
+        }
+    }
+    drain(true);
+}
+
 template <typename R>
 void launch_bvh_rebuild(const Dev<R>& d, cudaStream_t s, void* sortScratch, size_t, int keyBits) {
     if (d.nseg <= 0) return;
@@ -705,7 +838,10 @@ void launch_traverse(const Dev<R>& d, cudaStream_t s) {
     cudaMemsetAsync(d.numCols, 0, sizeof(int) * d.n, s);
     cudaMemsetAsync(d.travNext, 0, sizeof(unsigned), s);
     const int blocks = min((d.nseg + TRAV_THREADS - 1) / TRAV_THREADS, max(d.travBlocks, 1));
-    k_traverse<R><<<blocks, TRAV_THREADS, 0, s>>>(d);
+    if (d.travPacket)
+        k_traverse_packet<R><<<blocks, TRAV_THREADS, 0, s>>>(d);
+    else
+        k_traverse<R><<<blocks, TRAV_THREADS, 0, s>>>(d);
     k_lists<R><<<(d.nseg + 127) / 128, 128, 0, s>>>(d, 1);
 }
 
@@ -722,13 +858,15 @@ template void launch_bvh_refit<double>(const Dev<double>&, cudaStream_t);
 template void launch_bvh_reset<float>(const Dev<float>&, cudaStream_t);
 template void launch_bvh_reset<double>(const Dev<double>&, cudaStream_t);
 template <typename R>
-int traverse_blocks_per_sm() {
-    int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_traverse<R>, TRAV_THREADS, 0) != cudaSuccess || b < 1) {
+int traverse_blocks_per_sm() {  // resident blocks of both traversal kernels (the smaller)
+    int b = 0, c = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_traverse<R>, TRAV_THREADS, 0) != cudaSuccess || b < 1 ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_traverse_packet<R>, TRAV_THREADS, 0) != cudaSuccess ||
+        c < 1) {
         cudaGetLastError();
-        b = 4;
+        return 4;
     }
-    return b;
+    return b < c ? b : c;
 }
 template int traverse_blocks_per_sm<float>();
 template int traverse_blocks_per_sm<double>();

@@ -64,6 +64,7 @@ struct EngineBase {
     virtual yb_status drive_pins(double dt) = 0;
     virtual yb_status residual_substep(int type, double* out, int cap, int* count) = 0;
     virtual yb_status read_last_vel(double* out) = 0;
+    virtual void set_traversal(int packet) = 0;
 };
 
 }  // namespace
@@ -91,6 +92,7 @@ struct yb_sim {
     int iterLanes = 4;
     int iterPipe = 0;
     int useGraphs = 1;
+    int travPacket = 1;  // broadphase walk: 1 per warp of 32 queries, 0 per query
     uint64_t launches = 0;
     cudaStream_t stream = nullptr;     // active stream (own or the caller's)
     cudaStream_t ownStream = nullptr;  // created by configure, destroyed by yb_destroy
@@ -391,6 +393,7 @@ struct Engine : EngineBase {
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
             d.travBlocks = sms * traverse_blocks_per_sm<R>();
         }
+        d.travPacket = S->travPacket;
         YB_CUDA(cudaHostAlloc((void**)&spHost, sizeof(SceneParams<R>) * ns, cudaHostAllocDefault));
         YB_CUDA(cudaHostAlloc((void**)&errHost, sizeof(int) * EW_COUNT, cudaHostAllocDefault));
         YB_CUDA(cudaMemsetAsync(d.err, 0, sizeof(int) * EW_COUNT, S->stream));
@@ -814,6 +817,11 @@ struct Engine : EngineBase {
         if (e == cudaSuccess) e = cudaStreamSynchronize(S->stream);
         cudaFree(tmp);
         return cuda_status(e);
+    }
+
+    void set_traversal(int packet) override {
+        if (d.travPacket != packet) invalidate_graphs();
+        d.travPacket = packet;
     }
 
     yb_status read_last_vel(double* out) override {
@@ -1424,6 +1432,19 @@ yb_status yb_autotune(yb_sim* S, int32_t* bestThreads, int32_t* bestLanes, int32
     return st;
 }
 
+yb_status yb_set_traversal(yb_sim* S, int32_t packet) {
+    if (!S || (packet != 0 && packet != 1)) return YB_ERR_INVALID_ARGUMENT;
+    S->travPacket = packet;
+    if (S->eng) S->eng->set_traversal(packet);
+    return YB_OK;
+}
+
+yb_status yb_get_traversal(yb_sim* S, int32_t* packet) {
+    if (!S || !packet) return YB_ERR_INVALID_ARGUMENT;
+    *packet = S->travPacket;
+    return YB_OK;
+}
+
 yb_status yb_set_stream(yb_sim* S, void* stream) {
     if (!S) return YB_ERR_INVALID_ARGUMENT;
     if (S->stream) {
@@ -1711,6 +1732,7 @@ yb_status yb_batch_gather(int32_t count, yb_sim* const* srcSims, const int32_t* 
     S->iterThreads = srcSims[0]->iterThreads;
     S->iterLanes = srcSims[0]->iterLanes;
     S->iterPipe = srcSims[0]->iterPipe;
+    S->travPacket = srcSims[0]->travPacket;
     if (!S->configured) {
         cudaError_t e = cudaStreamCreateWithFlags(&S->ownStream, cudaStreamNonBlocking);
         if (e != cudaSuccess) {
@@ -1726,6 +1748,7 @@ yb_status yb_batch_gather(int32_t count, yb_sim* const* srcSims, const int32_t* 
         }
         S->configured = true;
     }
+    S->eng->set_traversal(S->travPacket);
     yb_status st = S->eng->gather(count, srcSims, srcScenes);
     if (st == YB_OK) st = validate_all_meta(S);
     if (st == YB_OK) S->eng->write_params();

@@ -381,6 +381,10 @@ class Sim:
         check(self._lib.yb_debug_dx(self._h, ptr(dx, ctypes.c_double)), "dx")
         return dx[:, :3].copy()
 
+    def set_traversal(self, packet=True):
+        """Broadphase walk: one per warp of 32 queries (packet) or one per query."""
+        check(self._lib.yb_set_traversal(self._h, 1 if packet else 0), "traversal")
+
     def debug_last_vel(self):
         lv = np.zeros((self.numVerts, 3))
         check(self._lib.yb_debug_last_vel(self._h, ptr(lv, ctypes.c_double)), "lastVel")
