@@ -62,6 +62,10 @@ def parse():
     p.add_argument("--every", type=int, default=30, help="twist: sample interval in frames")
     p.add_argument("--gravity", type=float, default=-9.8, help="twist: gravity along y (m/s^2)")
     p.add_argument("--budget-gb", type=float, default=120.0, help="serve: device-memory budget")
+    p.add_argument("--setup-threads", type=int, default=4, help="serve: host threads setting requests up")
+    p.add_argument("--max-batch-verts", type=int, default=8_000_000, help="serve: vertices per frame (0: budget only)")
+    p.add_argument("--drain", type=float, default=30.0, help="serve: seconds the admitted requests may finish in")
+    p.add_argument("--alone-sample", type=int, default=40, help="serve: requests timed alone")
     return p.parse_args()
 
 
@@ -471,37 +475,54 @@ def run_plain(spec, stream, shape):
 
 
 def run_serve(args):
-    """Serving loop: Poisson arrivals in real time, continuous batching on one GPU, against
-    the same requests served one at a time (FIFO) through plain per-request advance()."""
+    """Serving loop: Poisson arrivals in real time (config 5: --rate 200 --duration 60),
+    continuous batching on one GPU with request set-up on host threads overlapping the frames.
+    Arrivals stop after the window; the requests already in the batch then finish (no new
+    admissions, at most --drain seconds) and the rest of the queue is reported as not served.
+    Beside it, a sample of the same requests served one at a time through plain advance()."""
     import torch
 
     from yarnball_b200 import serve
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     reqs = serve.poisson_requests(args.rate, args.duration, frames=args.frames)
-    server = serve.Server(budget_bytes=args.budget_gb * 1e9, shape=(128, 0), stream=torch.cuda.Stream())
+    server = serve.Server(budget_bytes=args.budget_gb * 1e9, shape=(128, 0), stream=torch.cuda.Stream(),
+                          setup_threads=args.setup_threads, max_batch_vertices=args.max_batch_verts or None)
     pending = list(reqs)
     t0 = time.perf_counter()
-    while pending or server.busy():
+    while True:
         now = time.perf_counter() - t0
         while pending and pending[0].arrival <= now:
             server.submit(pending.pop(0))
-        if not server.busy() and pending:
+        in_window = now <= args.duration
+        if not in_window and (now > args.duration + args.drain or not any(
+                r.done_frames < r.frames for r in server.active)):
+            break
+        if not server.busy():
+            if not pending:
+                break
             time.sleep(max(0.0, pending[0].arrival - (time.perf_counter() - t0)))
             continue
-        server.step(now)
+        server.step(now, admit=in_window)
         done_t = time.perf_counter() - t0
         for r in server.finished:
             if r.finished_at is None:
                 r.finished_at = done_t
     wall = time.perf_counter() - t0
+    served_work = float(sum(server.frame_sizes)) * SUBSTEPS  # vertex-substeps advanced
+    arrived = [r for r in reqs if r.arrival <= min(wall, args.duration)]
+    done = [r for r in reqs if r.finished_at is not None]
+    lat = [r.finished_at - r.arrival for r in done]
+    wait = [r.admitted_at - r.arrival for r in done]
+    work = sum(r.vertices * SUBSTEPS * r.frames for r in done)
+    dev_s = sum(server.frame_ms) / 1e3
+    mean_req_work = float(np.mean([r.vertices * SUBSTEPS * r.frames for r in arrived])) if arrived else 0.0
+    queue_end = len(server.queue)
     server.close()
-    lat = [r.finished_at - r.arrival for r in reqs]
-    work = sum(r.vertices * SUBSTEPS * r.frames for r in reqs)
-    first, last = min(r.arrival for r in reqs), max(r.finished_at for r in reqs)
-    # the same requests, each alone, one after the other (FIFO single server)
+    # a sample of the same requests, each alone through plain advance(), one after the other
+    sample = arrived[: args.alone_sample]
     service = []
-    for r in reqs:
+    for r in sample:
         sim = serve.build_request_sim(r, (128, 0))
         st = torch.cuda.Stream()
         sim.set_stream(st.cuda_stream)
@@ -513,22 +534,29 @@ def run_serve(args):
         e1.synchronize()
         service.append(e0.elapsed_time(e1) / 1e3)
         sim.close()
-    tfree, lat_alone = 0.0, []
-    for r, sv in zip(reqs, service):
-        start = max(tfree, r.arrival)
-        tfree = start + sv
-        lat_alone.append(tfree - r.arrival)
+    alone_tp = sum(r.vertices * SUBSTEPS * r.frames for r in sample) / max(sum(service), 1e-9)
+    batched_tp = served_work / max(wall, 1e-9)
     out = {
         "metric": "serving: request latency and vertex-substeps/s under Poisson arrivals", "unit": "s",
-        "requests": len(reqs), "rate_per_s": args.rate, "arrival_window_s": args.duration,
-        "frames_per_request": args.frames, "budget_gb": args.budget_gb,
-        "request_latency_s": serve.percentiles(lat), "frame_latency_ms": serve.percentiles(server.frame_ms),
-        "frames": len(server.frame_ms), "max_batch_vertices": max(server.frame_sizes) if server.frame_sizes else 0,
-        "gathers": server.gathers, "throughput_vertex_substeps_per_s": work / (last - first), "wall_s": wall,
-        "alone": {"request_latency_s": serve.percentiles(lat_alone),
-                  "throughput_vertex_substeps_per_s": work / (tfree - first),
+        "rate_per_s": args.rate, "arrival_window_s": args.duration, "frames_per_request": args.frames,
+        "budget_gb": args.budget_gb, "max_batch_vertices": args.max_batch_verts or None,
+        "setup_threads": args.setup_threads,
+        "requests": {"arrived": len(arrived), "admitted": sum(1 for r in reqs if r.admitted_at is not None),
+                     "completed": len(done), "queued_at_end": queue_end},
+        "request_latency_s": serve.percentiles(lat), "queue_wait_s": serve.percentiles(wait),
+        "frame_latency_ms": serve.percentiles(server.frame_ms), "frames": len(server.frame_ms),
+        "batch_vertices": serve.percentiles([float(x) for x in server.frame_sizes]),
+        "queue_length": {"max": max(server.queue_lengths) if server.queue_lengths else 0, "end": queue_end},
+        "gathers": server.gathers,
+        "throughput_vertex_substeps_per_s": batched_tp,
+        "device_throughput_vertex_substeps_per_s": served_work / max(dev_s, 1e-9),
+        "completed_work_vertex_substeps": work, "wall_s": wall,
+        "offered_load_vertex_substeps_per_s": mean_req_work * args.rate,
+        "sustainable_rate_per_s": batched_tp / mean_req_work if mean_req_work else None,
+        "alone": {"requests": len(sample), "throughput_vertex_substeps_per_s": alone_tp,
                   "service_s": serve.percentiles(service)},
-        "request_vertices": serve.percentiles([r.vertices for r in reqs]),
+        "batched_over_alone": batched_tp / alone_tp if alone_tp else None,
+        "request_vertices": serve.percentiles([r.vertices for r in arrived]),
     }
     print(json.dumps(out))
 

@@ -5,9 +5,11 @@ scene that asks for a number of frames of 1/30 s.  The server keeps every admitt
 state on the device between frames and advances all of them with one batched advance() per
 frame, so requests of different sizes share every kernel launch:
 
-  * a request is set up on arrival (geometry, configure, upload) as a one-scene Sim;
-  * it is admitted at the next frame boundary if the device-memory budget allows (the
-    staging Sim and two batch allocations count against it), else it waits in a FIFO queue;
+  * a request waits in a FIFO queue; host threads set the head of the queue up (geometry,
+    configure, upload) as one-scene Sims while the frames run, a bounded number of vertices
+    ahead, so set-up overlaps device work;
+  * a set-up request is admitted at the next frame boundary if the device-memory budget (the
+    staged Sims and two batch allocations) and the optional per-frame vertex cap allow;
   * when membership changes, the batch is rebuilt by copying every remaining and newly
     admitted scene device to device (yb_batch_gather), reusing the previous batch's
     allocation when it is large enough (two allocations alternate);
@@ -19,7 +21,7 @@ shape), which tests/test_gpu_serving.py checks.
 """
 import collections
 import math
-import time
+from concurrent.futures import Future, ThreadPoolExecutor
 
 import numpy as np
 
@@ -38,6 +40,7 @@ class Request:
         self.seed = seed
         self.done_frames = 0
         self.staging = None           # one-scene Sim until admitted
+        self.future = None            # its set-up on a host thread
         self.admitted_at = None
         self.finished_at = None
         self.result = None            # (positions, velocities, rotors) after the last frame
@@ -76,13 +79,27 @@ def run_alone(req, shape=None):
 
 
 class Server:
+    """Continuous batching on one GPU.
+
+    budget_bytes        device memory for the batch (two allocations, gathered alternately)
+                        and the requests staged ahead of admission
+    max_batch_vertices  optional cap on the vertices advanced per frame: it bounds the frame
+                        latency (a frame's time grows with the batch) at the price of queueing
+    setup_threads       host threads that set requests up (geometry, configure, upload) ahead
+                        of admission, while frames run; 0 sets them up on the frame thread
+    prefetch_vertices   how many vertices of queued requests may be staged ahead
+    """
+
     def __init__(self, budget_bytes=120e9, shape=(128, 0), bytes_per_vertex=None, capacity_headroom=1.25,
-                 stream=None):
+                 stream=None, setup_threads=4, prefetch_vertices=4_000_000, max_batch_vertices=None):
         self.budget = float(budget_bytes)
         self.shape = shape
         self.bpv = bytes_per_vertex
         self.headroom = capacity_headroom
         self.stream = stream
+        self.prefetch = int(prefetch_vertices)
+        self.max_batch = max_batch_vertices
+        self.pool = ThreadPoolExecutor(setup_threads) if setup_threads > 0 else None
         self.queue = collections.deque()
         self.active = []              # requests in batch scene order
         self.batch = None
@@ -90,6 +107,7 @@ class Server:
         self.finished = []
         self.frame_ms = []            # device time of each batched frame
         self.frame_sizes = []         # vertices advanced in each frame
+        self.queue_lengths = []       # queued requests at each frame boundary
         self.gathers = 0
 
     # ---- memory accounting -------------------------------------------------------------
@@ -98,35 +116,59 @@ class Server:
             self.bpv = sim.device_bytes() / max(sim.numVerts, 1)
         return self.bpv
 
-    def _in_use(self):
-        verts = sum(r.vertices for r in self.active)
-        staged = sum(r.vertices for r in self.queue if r.staging is not None)
-        cap = 0
-        for b in (self.batch, self.spare):
-            if b is not None:
-                cap += b.device_bytes()
-        return cap + staged * (self.bpv or 0), verts
+    def _staged_vertices(self):
+        return sum(r.vertices for r in self.queue if r.future is not None)
 
     # ---- request flow ---------------------------------------------------------------
     def submit(self, req):
-        req.staging = build_request_sim(req, self.shape)
-        self._bytes_per_vertex(req.staging)
+        """Queues a request; its set-up starts on a host thread when the prefetch window allows."""
+        req.future = None
         self.queue.append(req)
+        self._stage()
+
+    def _stage(self):
+        staged = self._staged_vertices()
+        for r in self.queue:  # FIFO: stage the head of the queue first
+            if r.future is not None:
+                continue
+            if staged > 0 and staged + r.vertices > self.prefetch:
+                break
+            if self.pool is None:
+                f = Future()
+                f.set_result(build_request_sim(r, self.shape))
+                r.future = f
+            else:
+                r.future = self.pool.submit(build_request_sim, r, self.shape)
+            staged += r.vertices
 
     def _admit(self):
         joined = []
-        used, verts = self._in_use()
+        verts = sum(r.vertices for r in self.active)
         while self.queue:
             r = self.queue[0]
-            # two batch allocations of the grown size must fit, with the staged scenes
-            need = 2 * self.headroom * (verts + r.vertices) * self.bpv
+            if r.future is None:
+                break
+            if not r.future.done() and (self.active or joined):
+                break  # not set up yet: the batch goes on without it
+            sim = r.future.result()  # an idle server waits for its next request
+            self._bytes_per_vertex(sim)
             if self.active or joined:
-                if need > self.budget:
+                # two batch allocations of the grown size must fit the budget with the staged scenes
+                need = (2 * self.headroom * (verts + r.vertices) + self._staged_vertices()) * self.bpv
+                if need > self.budget or (self.max_batch and verts + r.vertices > self.max_batch):
                     break
             self.queue.popleft()
+            r.staging = sim
             joined.append(r)
             verts += r.vertices
+        self._stage()
         return joined
+
+    def _close_later(self, sim):
+        if self.pool is None:
+            sim.close()
+        else:
+            self.pool.submit(sim.close)
 
     def _regather(self, keep, joined):
         sources = [(self.batch, i) for i in keep] + [(r.staging, 0) for r in joined]
@@ -140,21 +182,23 @@ class Server:
         new = Sim.gather(sources, recycle=self.spare, capacity=int(total * self.headroom))
         self.gathers += 1
         if self.spare is not None and new is not self.spare:
-            self.spare.close()
+            self._close_later(self.spare)
         self.spare = self.batch
         self.batch = new
         self.batch.set_tuning(self.shape[0], self.shape[1], True, len(self.shape) > 2 and self.shape[2])
         if self.stream is not None:
             self.batch.set_stream(self.stream.cuda_stream)
-        for r in joined:
-            r.staging.close()
+        for r in joined:  # gather has finished its copies: the staging copies can go
+            self._close_later(r.staging)
             r.staging = None
         self.active = members
 
-    def step(self, now):
-        """One frame boundary: retire, admit, re-gather if needed, advance one frame."""
+    def step(self, now, admit=True):
+        """One frame boundary: retire, admit (unless admit is False), re-gather if needed,
+        advance one frame."""
+        self.queue_lengths.append(len(self.queue))
         keep = [i for i, r in enumerate(self.active) if r.done_frames < r.frames]
-        joined = self._admit()
+        joined = self._admit() if admit else []
         for r in joined:
             r.admitted_at = now
         if len(keep) != len(self.active) or joined:
@@ -190,12 +234,14 @@ class Server:
         return bool(self.queue) or any(r.done_frames < r.frames for r in self.active)
 
     def close(self):
+        if self.pool is not None:
+            self.pool.shutdown(wait=True)
         for b in (self.batch, self.spare):
             if b is not None:
                 b.close()
         for r in self.queue:
-            if r.staging is not None:
-                r.staging.close()
+            if r.future is not None:
+                r.future.result().close()
         self.batch = self.spare = None
 
 
