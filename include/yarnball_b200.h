@@ -184,7 +184,7 @@ const char* yb_status_string(yb_status s);
  * software pipelining of the contact loop (with lanes 0: flatten per warp instead of per
  * block); valid shapes: (128, 0, 0|1), (128|256, 1, 0|1), (256, 2, 0), (256, 4, 0|1),
  * (512, 4, 0), (256|512, 8, 0).  useGraphs: replay captured CUDA graphs per substep.
- * Default (256, 4, 0), graphs on. */
+ * Default (128, 0, 0), the load-balanced kernel, graphs on. */
 yb_status yb_set_tuning(yb_sim* sim, int32_t iterThreads, int32_t lanesPerVertex, int32_t pipelined,
                         int32_t useGraphs);
 yb_status yb_get_tuning(yb_sim* sim, int32_t* iterThreads, int32_t* lanesPerVertex, int32_t* pipelined,
@@ -201,6 +201,12 @@ yb_status yb_autotune(yb_sim* sim, int32_t* bestThreads, int32_t* bestLanes, int
  * consecutive queries, packet = 0 once per query.  The contact lists are identical. */
 yb_status yb_set_traversal(yb_sim* sim, int32_t packet);
 yb_status yb_get_traversal(yb_sim* sim, int32_t* packet);
+
+/* Simulations of at most 256 vertices advance all substeps of an advance() in one launch of a
+ * one-block kernel (enable = 1, the default); enable = 0 uses the multi-block kernels and the
+ * BVH.  The results are the same bit for bit with the load-balanced Newton kernel (tuning
+ * lanesPerVertex 0, pipelined 0). */
+yb_status yb_set_small_path(yb_sim* sim, int32_t enable);
 
 /* Launch the simulation's work on `stream` (a cudaStream_t; NULL returns to the simulation's
  * own stream).  Lets a caller order the engine with its own work and time it with events. */

@@ -146,6 +146,7 @@ SIGNATURES = {
     "yb_debug_dx": (ctypes.c_int, [_P, c_double_p]),
     "yb_debug_last_vel": (ctypes.c_int, [_P, c_double_p]),
     "yb_set_traversal": (ctypes.c_int, [_P, ctypes.c_int32]),
+    "yb_set_small_path": (ctypes.c_int, [_P, ctypes.c_int32]),
     "yb_get_traversal": (ctypes.c_int, [_P, c_int32_p]),
     "yb_debug_phases": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_float]),
     "yb_debug_sort_pairs": (ctypes.c_int, [c_uint64_p, c_int32_p, ctypes.c_int32, ctypes.c_int32, c_uint64_p,

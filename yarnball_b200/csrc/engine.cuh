@@ -189,6 +189,12 @@ template <typename R>
 void launch_pin_drive(const Dev<R>& d, const float4* init, const unsigned char* group, const PinMotion* m, double dt,
                       cudaStream_t s);  // scene roots := empty
 
+// One block advances a small simulation (n <= 256 vertices) through `steps` substeps in one launch.
+template <typename R> bool small_path_fits(const Dev<R>& d);
+template <typename R>
+void launch_small(const Dev<R>& d, int steps, int numItr, unsigned long long step0, int detectionPeriod, bool kahan,
+                  cudaStream_t s);
+
 // Radix sort of (u64 key, int value) pairs, ascending by the low `bits` key bits, stable.
 // keys/vals ping-pong between [0] and [1]; the result lands in buffer (passes & 1).
 size_t radix_sort_scratch_bytes(int n);

@@ -65,6 +65,8 @@ struct EngineBase {
     virtual yb_status residual_substep(int type, double* out, int cap, int* count) = 0;
     virtual yb_status read_last_vel(double* out) = 0;
     virtual void set_traversal(int packet) = 0;
+    virtual bool small_fits() const = 0;
+    virtual yb_status run_small(int steps) = 0;
 };
 
 }  // namespace
@@ -88,11 +90,12 @@ struct yb_sim {
     float lastBVHRebuild = INFINITY;
     uint64_t stepCounter = 0;
     int lastErrorCode = 0, lastWarningCode = 0;
-    int iterThreads = 256;
-    int iterLanes = 4;
+    int iterThreads = 128;
+    int iterLanes = 0;
     int iterPipe = 0;
     int useGraphs = 1;
     int travPacket = 1;  // broadphase walk: 1 per warp of 32 queries, 0 per query
+    int useSmall = 1;    // advance small simulations with the one-block kernel
     uint64_t launches = 0;
     cudaStream_t stream = nullptr;     // active stream (own or the caller's)
     cudaStream_t ownStream = nullptr;  // created by configure, destroyed by yb_destroy
@@ -717,8 +720,9 @@ struct Engine : EngineBase {
         uint64_t k = 0;
         launch_init(d, st); k++;
         if (detect && d.nseg > 0) {
-            if (rebuild) {
+            if (rebuild) {  // the schedule rebuilds first after any path that did not use the tree
                 launch_bvh_rebuild(d, st, sortScratch, sortBytes, keyBits);
+                bvhBuilt = true;
                 const int passes = d.nseg > 1 ? (keyBits + 7) / 8 : 0;
                 k += 3 + (d.nseg > 1 ? 2 + passes : 0) + 1 + DEPTH_LAUNCHES + 2;
             } else {
@@ -819,6 +823,22 @@ struct Engine : EngineBase {
         return cuda_status(e);
     }
 
+    bool bvhBuilt = false;  // the tree exists (a refit needs one)
+
+    bool small_fits() const override { return small_path_fits(d); }
+
+    // All substeps of an advance in one launch of the one-block kernel; the BVH is not used,
+    // so the next detection on the multi-block path rebuilds it.
+    yb_status run_small(int steps) override {
+        launch_small(d, steps, num_itr(), (unsigned long long)S->stepCounter, S->meta[0].detectionPeriod,
+                     sizeof(R) == 4, S->stream);
+        S->launches++;
+        bvhBuilt = false;
+        S->lastBVHRebuild = INFINITY;
+        YB_CUDA(cudaGetLastError());
+        return YB_OK;
+    }
+
     void set_traversal(int packet) override {
         if (d.travPacket != packet) invalidate_graphs();
         d.travPacket = packet;
@@ -857,6 +877,10 @@ struct Engine : EngineBase {
     }
 
     yb_status bounds(int scene, float* out) override {
+        if (!bvhBuilt && d.nseg > 0) {  // the one-block path does not keep a tree: build one now
+            launch_bvh_rebuild(d, S->stream, sortScratch, sortBytes, keyBits);
+            bvhBuilt = true;
+        }
         launch_scene_root_box(d, rootBoxes, S->stream);
         S->launches++;
         std::vector<float> b(6 * (size_t)S->numScenes);
@@ -910,9 +934,10 @@ struct Engine : EngineBase {
         mark(0);
         launch_init(d, st); launches[0]++;
         if (detect && d.nseg > 0) {
-            if (rebuild) {
+            if (rebuild || !bvhBuilt) {
                 mark(1);
                 launch_bvh_rebuild(d, st, sortScratch, sortBytes, keyBits);
+                bvhBuilt = true;
                 const int passes = d.nseg > 1 ? (keyBits + 7) / 8 : 0;
                 launches[1] += 3 + (d.nseg > 1 ? 2 + passes : 0) + 1 + DEPTH_LAUNCHES + 2;
             } else {
@@ -998,8 +1023,9 @@ struct Engine : EngineBase {
         uint64_t k = 0;
         if (mask & 1) { launch_init(d, st); k++; buf = 0; }
         if ((mask & 6) && d.nseg > 0) {
-            if (mask & 2) {
+            if ((mask & 2) || !bvhBuilt) {  // a refit needs a tree
                 launch_bvh_rebuild(d, st, sortScratch, sortBytes, keyBits);
+                bvhBuilt = true;
                 k += 3 + (d.nseg > 1 ? 2 + (keyBits + 7) / 8 : 0) + 1 + DEPTH_LAUNCHES + 2;
             } else {
                 launch_bvh_refit(d, st);
@@ -1273,6 +1299,16 @@ yb_status yb_advance(yb_sim* S, float dt, float* advanced) {
     st = S->eng->drive_pins(dt);
     if (st != YB_OK) return st;
     const yb_meta& m0 = S->meta[0];
+    if (S->useSmall && S->eng->small_fits()) {
+        // a small simulation: every substep in one launch of the one-block kernel
+        st = S->eng->run_small(steps);
+        if (st != YB_OK) return st;
+        S->stepCounter += (uint64_t)steps;
+        for (auto& m : S->meta) m.time += dt;
+        st = S->eng->check_errors();
+        if (advanced) *advanced = dt;
+        return st;
+    }
     for (int s = 0; s < steps; s++, S->stepCounter++) {
         int type = 2;
         if (m0.detectionPeriod > 0 && S->stepCounter % (uint64_t)m0.detectionPeriod == 0) {
@@ -1430,6 +1466,12 @@ yb_status yb_autotune(yb_sim* S, int32_t* bestThreads, int32_t* bestLanes, int32
     if (bestPipelined) *bestPipelined = bp;
     if (bestMs) *bestMs = best;
     return st;
+}
+
+yb_status yb_set_small_path(yb_sim* S, int32_t enable) {
+    if (!S || (enable != 0 && enable != 1)) return YB_ERR_INVALID_ARGUMENT;
+    S->useSmall = enable;
+    return YB_OK;
 }
 
 yb_status yb_set_traversal(yb_sim* S, int32_t packet) {
@@ -1733,6 +1775,7 @@ yb_status yb_batch_gather(int32_t count, yb_sim* const* srcSims, const int32_t* 
     S->iterLanes = srcSims[0]->iterLanes;
     S->iterPipe = srcSims[0]->iterPipe;
     S->travPacket = srcSims[0]->travPacket;
+    S->useSmall = srcSims[0]->useSmall;
     if (!S->configured) {
         cudaError_t e = cudaStreamCreateWithFlags(&S->ownStream, cudaStreamNonBlocking);
         if (e != cudaSuccess) {

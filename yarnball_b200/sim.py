@@ -222,7 +222,7 @@ class Sim:
         return np.ctypeslib.as_array(p, shape=(c.value,)).copy()
 
     # ---- additions -------------------------------------------------------------------
-    def set_tuning(self, iterThreads=256, lanesPerVertex=4, useGraphs=True, pipelined=False):
+    def set_tuning(self, iterThreads=128, lanesPerVertex=0, useGraphs=True, pipelined=False):
         check(self._lib.yb_set_tuning(self._h, int(iterThreads), int(lanesPerVertex), 1 if pipelined else 0,
                                       1 if useGraphs else 0), "tuning")
 
@@ -380,6 +380,11 @@ class Sim:
         dx = np.zeros((self.numVerts, 4))
         check(self._lib.yb_debug_dx(self._h, ptr(dx, ctypes.c_double)), "dx")
         return dx[:, :3].copy()
+
+    def set_small_path(self, enable=True):
+        """Advance simulations of at most 256 vertices with the one-block kernel (one launch
+        per advance)."""
+        check(self._lib.yb_set_small_path(self._h, 1 if enable else 0), "small path")
 
     def set_traversal(self, packet=True):
         """Broadphase walk: one per warp of 32 queries (packet) or one per query."""
