@@ -21,6 +21,7 @@ shape), which tests/test_gpu_serving.py checks.
 """
 import collections
 import math
+import threading
 from concurrent.futures import Future, ThreadPoolExecutor
 
 import numpy as np
@@ -47,12 +48,25 @@ class Request:
         self.vertices = int(np.sum(spec[0]))
 
 
-def build_request_sim(req, shape=None, meta=None):
-    lens, kbend = req.spec
-    lens = np.asarray(lens, np.int32)
+# Device work of the set-up threads (allocation, configure, upload, release) and the frame
+# thread's batch work (gather, advance with its graph capture, download) never overlap: a
+# stream capture must not see another thread's allocation or release, which may synchronise
+# the device.  The host part of a set-up (the geometry) runs outside the lock, beside frames.
+_device_lock = threading.Lock()
+
+
+def request_geometry(req):
+    lens = np.asarray(req.spec[0], np.int32)
     # pile density at most that of the 1024 x 256 pile in a 10 cm cube
     cube = scenes.CUBE * max(1.0, lens.sum() / 262144.0) ** (1.0 / 3.0)
-    pos = scenes.random_walks(req.seed, lens, cube=cube)
+    return scenes.random_walks(req.seed, lens, cube=cube)
+
+
+def build_request_sim(req, shape=None, meta=None, pos=None):
+    lens, kbend = req.spec
+    lens = np.asarray(lens, np.int32)
+    if pos is None:
+        pos = request_geometry(req)
     sim = Sim(int(lens.sum()))
     scenes.fill_yarns(sim, pos, lens, pin_first=True)
     for k, v in dict(scenes.PILE_META, **(meta or {})).items():
@@ -138,8 +152,13 @@ class Server:
                 f.set_result(build_request_sim(r, self.shape))
                 r.future = f
             else:
-                r.future = self.pool.submit(build_request_sim, r, self.shape)
+                r.future = self.pool.submit(self._set_up, r)
             staged += r.vertices
+
+    def _set_up(self, r):
+        pos = request_geometry(r)  # host work, beside the frames
+        with _device_lock:
+            return build_request_sim(r, self.shape, pos=pos)
 
     def _admit(self):
         joined = []
@@ -148,9 +167,9 @@ class Server:
             r = self.queue[0]
             if r.future is None:
                 break
-            if not r.future.done() and (self.active or joined):
+            if not r.future.done():
                 break  # not set up yet: the batch goes on without it
-            sim = r.future.result()  # an idle server waits for its next request
+            sim = r.future.result()
             self._bytes_per_vertex(sim)
             if self.active or joined:
                 # two batch allocations of the grown size must fit the budget with the staged scenes
@@ -168,7 +187,12 @@ class Server:
         if self.pool is None:
             sim.close()
         else:
-            self.pool.submit(sim.close)
+            self.pool.submit(self._release, sim)
+
+    @staticmethod
+    def _release(sim):
+        with _device_lock:
+            sim.close()
 
     def _regather(self, keep, joined):
         sources = [(self.batch, i) for i in keep] + [(r.staging, 0) for r in joined]
@@ -196,6 +220,12 @@ class Server:
     def step(self, now, admit=True):
         """One frame boundary: retire, admit (unless admit is False), re-gather if needed,
         advance one frame."""
+        if admit and not self.active and self.queue and self.queue[0].future is not None:
+            self.queue[0].future.result()  # an idle server waits for its next request (unlocked)
+        with _device_lock:
+            return self._step(now, admit)
+
+    def _step(self, now, admit):
         self.queue_lengths.append(len(self.queue))
         keep = [i for i, r in enumerate(self.active) if r.done_frames < r.frames]
         joined = self._admit() if admit else []
