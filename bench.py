@@ -325,13 +325,18 @@ def run_ours(args):
     achieved = bytes_per_launch / (iter_ms / 1e3) / 1e9
     peak, peak_kind = load_peaks()
     tr = load_traffic()
-    traffic = None
-    if tr:
+    traffic, traffic_src = None, None
+    if tr and tr.get("vertices") == n:
+        traffic = tr["dram_bytes_per_launch"]  # captured on this very workload
+        traffic_src = "ncu capture of one launch of this workload (%s)" % tr["summary"]
+    elif tr:
         traffic = tr["dram_bytes_per_vertex"] * n
+        traffic_src = "ncu capture at %d vertices scaled by the vertex count (%s)" % (tr["vertices"], tr["summary"])
     prof_total = sum(prof_ms.values())
     roofline = {
         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-        "traffic": traffic, "kernel": "k_iter (fused Newton position solve + orientation update)",
+        "traffic": traffic, "traffic_source": traffic_src,
+        "kernel": "k_iter (fused Newton position solve + orientation update)",
         "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
         "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": iter_ms, "cbar": cbar,
         "kernel_share": {k: v / prof_total for k, v in prof_ms.items()},

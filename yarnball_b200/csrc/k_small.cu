@@ -34,6 +34,7 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_small(Dev<R> d, int steps, in
     __shared__ R sHb[6][SMALL_THREADS];
     __shared__ R sSL[SMALL_THREADS];
     __shared__ R sDX[3][SMALL_THREADS];
+    typedef Ex<R> E;
     const int k = threadIdx.x;
     const int n = d.n;
     const bool valid = k < n;
@@ -148,12 +149,15 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_small(Dev<R> d, int steps, in
                     cHa.zero();
                     cHb.zero();
                     contact_term(e, dx, dx1, r0, r1, xyz(pd.a), xyz(pd.b), sp, cfa, cHa, cfb, cHb);
-                    fa += cfa;
-                    fb += cfb;
+                    // Separately rounded sums: k_iter_bal adds each contribution after a trip
+                    // through shared memory, so the compiler cannot fuse the contribution's last
+                    // multiply into the sum there; it must not here either.
+                    fa = V3<R>(E::add(fa.x, cfa.x), E::add(fa.y, cfa.y), E::add(fa.z, cfa.z));
+                    fb = V3<R>(E::add(fb.x, cfb.x), E::add(fb.y, cfb.y), E::add(fb.z, cfb.z));
 #pragma unroll
                     for (int q = 0; q < 6; q++) {
-                        Ha.d[q] += cHa.d[q];
-                        Hb.d[q] += cHb.d[q];
+                        Ha.d[q] = E::add(Ha.d[q], cHa.d[q]);
+                        Hb.d[q] = E::add(Hb.d[q], cHb.d[q]);
                     }
                 }
             }
