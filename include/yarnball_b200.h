@@ -204,8 +204,9 @@ yb_status yb_get_traversal(yb_sim* sim, int32_t* packet);
 
 /* Simulations of at most 256 vertices advance all substeps of an advance() in one launch of a
  * one-block kernel (enable = 1, the default); enable = 0 uses the multi-block kernels and the
- * BVH.  The results are the same bit for bit with the load-balanced Newton kernel (tuning
- * lanesPerVertex 0, pipelined 0). */
+ * BVH.  Both run the same device functions in the same order (the load-balanced Newton
+ * kernel's summation order); they agree to rounding, since the compiler may fuse multiply-adds
+ * differently inside the one kernel. */
 yb_status yb_set_small_path(yb_sim* sim, int32_t enable);
 
 /* Launch the simulation's work on `stream` (a cudaStream_t; NULL returns to the simulation's

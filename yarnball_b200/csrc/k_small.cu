@@ -6,10 +6,12 @@
 // launches, advection) is bound by launch latency: the README two-yarn scene (64 vertices)
 // takes ~64 us per substep that way.  Here one block of SMALL_THREADS threads, one vertex per
 // thread, runs all substeps with block barriers between the phases: the same device functions
-// as the multi-block kernels (step.cuh, detect.cuh) in the same order, so the results are
-// bit-identical to the multi-block path with the load-balanced Newton kernel, and the contact
-// set is the same (every pair of segments goes through the narrow-phase filter; the filter
-// keeps only pairs whose padded boxes overlap, which is all the BVH query contributes).
+// as the multi-block kernels (step.cuh, detect.cuh) in the same order and with the
+// load-balanced Newton kernel's summation order, and the same contact set (every pair of
+// segments goes through the narrow-phase filter; a pair the filter keeps has overlapping padded
+// boxes, which is all the BVH query contributes).  The compiler may contract multiplies and
+// adds into fused operations differently in this one kernel than in the separate kernels, so
+// the two paths agree to rounding rather than bit for bit.
 //
 // Reference semantics: Sim::advance (sim/step.cpp:36-55) with initItr / endItr
 // (sim/iteration.cu), detectCollisions + buildCollisionList (sim/collision.cu:39-119),

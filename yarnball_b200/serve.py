@@ -17,7 +17,9 @@ frame, so requests of different sizes share every kernel launch:
 
 Because a scene's state travels with it and every substep re-detects contacts, a scene
 gives bit-identical results alone and inside any mix (detectionPeriod 1, same Newton kernel
-shape), which tests/test_gpu_serving.py checks.
+shape, multi-block kernels), which tests/test_gpu_serving.py checks.  A scene of at most 256
+vertices simulated alone takes the one-block small-simulation path instead, which agrees with
+the multi-block kernels to rounding.
 """
 import collections
 import math
