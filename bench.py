@@ -62,7 +62,7 @@ def parse():
     p.add_argument("--every", type=int, default=30, help="twist: sample interval in frames")
     p.add_argument("--gravity", type=float, default=-9.8, help="twist: gravity along y (m/s^2)")
     p.add_argument("--budget-gb", type=float, default=120.0, help="serve: device-memory budget")
-    p.add_argument("--setup-threads", type=int, default=4, help="serve: host threads setting requests up")
+    p.add_argument("--setup-threads", type=int, default=4, help="serve: host threads generating request geometry")
     p.add_argument("--max-batch-verts", type=int, default=8_000_000, help="serve: vertices per frame (0: budget only)")
     p.add_argument("--drain", type=float, default=30.0, help="serve: seconds the admitted requests may finish in")
     p.add_argument("--alone-sample", type=int, default=40, help="serve: requests timed alone")
@@ -481,7 +481,8 @@ def run_plain(spec, stream, shape):
 
 def run_serve(args):
     """Serving loop: Poisson arrivals in real time (config 5: --rate 200 --duration 60),
-    continuous batching on one GPU with request set-up on host threads overlapping the frames.
+    continuous batching on one GPU with request geometry generated on host threads while the
+    frames run (the frame thread makes every CUDA call).
     Arrivals stop after the window; the requests already in the batch then finish (no new
     admissions, at most --drain seconds) and the rest of the queue is reported as not served.
     Beside it, a sample of the same requests served one at a time through plain advance()."""

@@ -74,9 +74,11 @@ __device__ __forceinline__ bool pair_keep(const Dev<R>& d, int x, int y, const S
 // Step-size limit (collision.cu:121-159), split so that contacts can be spread over threads:
 // step_limit_base is the per-segment start value, contact_step_limit one contact's bound
 // 0.45 x centre-line distance.  A contact also stages the partner's endpoints relative to p0
-// (for c < RELCAP, read by every Newton iteration of the substep), reports an
-// interpenetration (distance at or below 2 radius, each unordered pair once, o > k) and
-// returns the centre-line distance in dist.
+// in slot `stage` of relA/relB (read by every Newton iteration of the substep; NO_STAGE: not
+// staged), reports an interpenetration (distance at or below 2 radius, each unordered pair
+// once, o > k) and returns the centre-line distance in dist.
+constexpr size_t NO_STAGE = ~(size_t)0;
+
 template <typename R>
 __device__ __forceinline__ R step_limit_base(const Dev<R>& d, int k, const SceneParams<R>& sp) {
     typedef Ex<R> E;
@@ -86,18 +88,17 @@ __device__ __forceinline__ R step_limit_base(const Dev<R>& d, int k, const Scene
 }
 
 template <typename R>
-__device__ __forceinline__ R contact_step_limit(const Dev<R>& d, int k, int c, int o, const V3<R>& a0,
+__device__ __forceinline__ R contact_step_limit(const Dev<R>& d, int k, size_t stage, int o, const V3<R>& a0,
                                                 const V3<R>& a1, const SceneParams<R>& sp, bool& pen, R& dist) {
     typedef Ex<R> E;
     const V3<R> b0 = xsub(xyz(d.pos[o]), a0);
     const V3<R> b1 = xsub(xyz(d.pos[o + 1]), a0);
-    if (c < RELCAP) {
-        const size_t at = rel_at(k, c);
-        d.relA[at] = v4(b0, b1.x);
+    if (stage != NO_STAGE) {
+        d.relA[stage] = v4(b0, b1.x);
         R2<R> rb;
         rb.x = b1.y;
         rb.y = b1.z;
-        d.relB[at] = rb;
+        d.relB[stage] = rb;
     }
     const UVT<R> uv = closest_uv_exact(a1, b0, b1);
     const V3<R> nrm = xsub(xscale(uv.u, a1), xmix(b0, b1, uv.v));

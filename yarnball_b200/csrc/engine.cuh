@@ -13,7 +13,12 @@
 //   stepLim  R      per-segment displacement limit (collision.cu:121-159)
 //   numCols  int    contacts of each segment
 //   cols     int    contact partner ids, one row per segment: cols[seg * MAX_COLS + k]
-//   relA/B   V4,R2  partner endpoints relative to p0 for the first RELCAP contacts
+//                   (the broadphase appends here; the list pass sorts each row)
+//   csrOff   u32    n + 1: the contacts of vertex k, packed in vertex order by the list pass
+//                   every substep, are slots [csrOff[k], csrOff[k+1]) of
+//   csrCols  int    partner ids (sorted within each vertex's range)
+//   relA/B   V4,R2  partner endpoints relative to p0, staged per substep in the same slots
+//                   while the slot is below relCap (the one-block path stages rows of RELCAP)
 // Segments are the vertices with hasNext; segs[] lists them and is the leaf set of the BVH.
 #pragma once
 #include "ybmath.cuh"
@@ -43,7 +48,7 @@ enum {
                          // at substep start (cumulative min; +inf before the first contact)
     EW_COUNT = 8
 };
-enum { IE_BVH_STACK = 1, IE_SORT_WAIT = 2, IE_GRID_WAIT = 4, IE_REFIT = 8 };
+enum { IE_BVH_STACK = 1, IE_SORT_WAIT = 2, IE_GRID_WAIT = 4, IE_REFIT = 8, IE_LIST_WAIT = 16, IE_CONTACT = 32 };
 
 // The Newton iterate of vertex k stored together with that of vertex k+1, so that a segment's
 // two endpoints come from one 32-byte sector (one gather per contact partner).
@@ -58,7 +63,8 @@ struct alignas(sizeof(R) * 2) R2 {
     R x, y;
 };
 
-constexpr int RELCAP = 8;  // contacts per segment with staged relative partner positions
+constexpr int RELCAP = 8;  // staged relative partner positions: RELCAP x vertices slots in all
+constexpr int LIST_THREADS = 128;  // vertices per block of the list pass (one packed-offset tile)
 
 // Wide records are built only for the nodes the walk loads: those at an even depth below
 // their scene's root (a record's entries are grandchildren).  Depths come from pointer jumping
@@ -148,8 +154,13 @@ struct Dev {
     R* stepLim;
     int* numCols;
     int* cols;
-    V4<R>* relA;      // staged per substep for contacts c < RELCAP, one row per segment [seg*RELCAP + c]:
+    V4<R>* relA;      // staged per substep in the packed slots below relCap:
     R2<R>* relB;      //   relA = (b0 - p0, (b1 - p0).x), relB = (b1 - p0).yz
+    unsigned* csrOff; // n + 1 packed offsets (see the layout above)
+    int* csrCols;     // csrCap packed partner ids
+    unsigned csrCap;  // slots of csrCols
+    unsigned relCap;  // slots of relA / relB
+    unsigned long long* listStatus;  // list pass: [0] tile ticket, [1 + tile] look-back status
     int* segs;        // segment -> vertex index, ascending (scene-contiguous)
     const SceneParams<R>* sp;
     int* err;         // EW_COUNT ints

@@ -556,52 +556,56 @@ __device__ __forceinline__ void sort_list(const Dev<R>& d, int k, int n) {
     }
 }
 
-// Per segment after the broadphase: clamp and check the count, sort the list by partner id
-// (fixed summation order in the Newton iteration), then the step-size limit.  With
-// sortLists = 0 it only recomputes the step limit from the existing lists (substeps without
-// detection, collision.cu:121-172).  A block of 128 segments flattens their contact lists
-// (block scan) and evaluates 128 contacts at a time, one per thread; each segment then takes
-// the minimum over its contacts in list order (the minimum is exact, so this equals a
-// per-segment loop).
+// List pass, every substep, over tiles of LIST_THREADS consecutive vertices.  Per segment after
+// the broadphase: clamp and check the count, sort the list by partner id (fixed summation order
+// in the Newton iteration); with sortLists = 0 the lists are kept (substeps without detection,
+// collision.cu:121-172).  Then the lists of all vertices are packed in vertex order (csrOff,
+// csrCols): a tile takes its index from a ticket counter, scans its counts and resolves its
+// first slot by decoupled look-back over the tiles before it (which hold smaller tickets, so
+// they are running or done; each wait is bounded and a timeout sets IE_LIST_WAIT).  The tile's
+// contacts are then evaluated 128 at a time, one per thread: the packed partner id, the
+// partner endpoints staged relative to p0 in the same slot, and the step-size limit
+// (collision.cu:121-159), of which each segment takes the minimum over its contacts in list
+// order (the minimum is exact, so this equals a per-segment loop).  The packed slots are
+// contiguous per tile, so the Newton iteration reads them coalesced.
+constexpr int LIST_SPIN_LIMIT = 1 << 22;
+constexpr unsigned long long LS_AGG = 1ull << 62;
+constexpr unsigned long long LS_PRE = 2ull << 62;
+constexpr unsigned long long LS_VAL = (1ull << 62) - 1;
+
 template <typename R>
-__global__ void __launch_bounds__(128) k_lists(Dev<R> d, int sortLists) {
-    constexpr int B = 128;
+__global__ void __launch_bounds__(LIST_THREADS) k_lists(Dev<R> d, int sortLists) {
+    constexpr int B = LIST_THREADS;
     __shared__ int sOff[B + 1];
     __shared__ int sWarp[B / 32];
-    __shared__ int sSeg[B];
+    __shared__ int sTile;
+    __shared__ unsigned long long sBase;
     __shared__ R sA0[3][B], sA1[3][B];
     __shared__ int sScene[B];
     __shared__ R sLim[B];
     const int t = threadIdx.x;
-    const int si = blockIdx.x * B + t;
-    const bool valid = si < d.nseg;
-    int k = -1, nc = 0, sc = 0, rawCount = 0;
+    if (t == 0) sTile = (int)atomicAdd(d.listStatus, 1ull);
+    __syncthreads();
+    const int tile = sTile;
+    const int k = tile * B + t;
+    const bool inRange = k < d.n;
+    bool valid = false;  // k is a segment
+    int nc = 0, sc = 0, rawCount = 0;
     V3<R> a0(R(0)), a1(R(0));
-    if (valid) {
-        k = d.segs[si];
-        sc = scene_of(d.vp[k].flags);
-        nc = d.numCols[k];
-        rawCount = nc;
-        if (sortLists) {
-            if (nc > MAX_COLS) d.err[EW_ERROR] = 1;
+    if (inRange) {
+        const uint32_t fl = d.vp[k].flags;
+        valid = (fl & F_HAS_NEXT) != 0;
+        if (valid) {
+            sc = scene_of(fl);
+            nc = d.numCols[k];
+            rawCount = nc;
+            if (sortLists && nc > MAX_COLS) d.err[EW_ERROR] = 1;
             nc = min(nc, MAX_COLS);
-            d.numCols[k] = nc;
+            if (sortLists) d.numCols[k] = nc;
+            a0 = xyz(d.pos[k]);
+            a1 = xsub(xyz(d.pos[k + 1]), a0);
         }
-        a0 = xyz(d.pos[k]);
-        a1 = xsub(xyz(d.pos[k + 1]), a0);
     }
-    if (sortLists) {
-        // largest list of the warp (before the clamp), one atomic per warp
-        int m = rawCount;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
-        if ((t & 31) == 0 && m) atomicMax(&d.err[EW_MAX_COLS], m);
-        sort_list(d, k, valid ? nc : 0);
-    }
-    sSeg[t] = k;
-    sScene[t] = sc;
-    sA0[0][t] = a0.x; sA0[1][t] = a0.y; sA0[2][t] = a0.z;
-    sA1[0][t] = a1.x; sA1[1][t] = a1.y; sA1[2][t] = a1.z;
     {
         const int lane = t & 31, w = t >> 5;
         int x = nc;
@@ -618,14 +622,62 @@ __global__ void __launch_bounds__(128) k_lists(Dev<R> d, int sortLists) {
         if (t == B - 1) sOff[B] = wo + x;
         __syncthreads();
     }
+    // The tile's count is published before the sort, so that a later tile's look-back rarely
+    // has to wait for it.
+    volatile unsigned long long* st = d.listStatus + 1;
+    if (t == 0) st[tile] = (tile == 0 ? LS_PRE : LS_AGG) | (unsigned long long)sOff[B];
+    if (sortLists) {
+        // largest list of the warp (before the clamp), one atomic per warp
+        int m = rawCount;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if ((t & 31) == 0 && m) atomicMax(&d.err[EW_MAX_COLS], m);
+        sort_list(d, valid ? k : -1, nc);
+    }
+    sScene[t] = sc;
+    sA0[0][t] = a0.x; sA0[1][t] = a0.y; sA0[2][t] = a0.z;
+    sA1[0][t] = a1.x; sA1[1][t] = a1.y; sA1[2][t] = a1.z;
+    // first packed slot of this tile: decoupled look-back (thread 0)
+    if (t == 0) {
+        const unsigned long long agg = (unsigned long long)sOff[B];
+        unsigned long long excl = 0;
+        if (tile > 0) {
+            bool timedOut = false;
+            for (int p = tile - 1; p >= 0; p--) {
+                unsigned long long w = st[p];
+                int spins = 0;
+                while ((w >> 62) == 0ull) {
+                    if (++spins > LIST_SPIN_LIMIT) {
+                        timedOut = true;
+                        break;
+                    }
+                    if (spins > 64) __nanosleep(32);
+                    w = st[p];
+                }
+                if (timedOut) break;
+                excl += w & LS_VAL;
+                if (w & LS_PRE) break;
+            }
+            if (timedOut) atomicOr(&d.err[EW_INTERNAL], IE_LIST_WAIT);
+            st[tile] = LS_PRE | (excl + agg);
+        }
+        if (excl + agg > (unsigned long long)d.csrCap) atomicOr(&d.err[EW_INTERNAL], IE_CONTACT);
+        sBase = excl;
+    }
+    __syncthreads();
+    const unsigned long long base = sBase;
     const int total = sOff[B];
     const int myOff = sOff[t];
+    if (inRange) {
+        d.csrOff[k] = (unsigned)(base + myOff);
+        if (k == d.n - 1) d.csrOff[d.n] = (unsigned)(base + myOff + nc);
+    }
     R m = R(0);
     if (valid) m = step_limit_base(d, k, d.sp[sc]);
     int pens = 0;
     float dmin = INFINITY;
-    for (int base = 0; base < total; base += B) {
-        const int f = base + t;
+    for (int b0 = 0; b0 < total; b0 += B) {
+        const int f = b0 + t;
         R lim = yinf<R>();
         if (f < total) {
             int lo = 0, hi = B - 1;  // owner: the last slot whose offset is <= f
@@ -634,20 +686,23 @@ __global__ void __launch_bounds__(128) k_lists(Dev<R> d, int sortLists) {
                 if (sOff[mid] <= f) lo = mid; else hi = mid - 1;
             }
             const int s = lo, c = f - sOff[s];
-            const int ks = sSeg[s];
+            const int ks = tile * B + s;
             const int o = d.cols[col_at(ks, c)];
+            const unsigned long long g = base + (unsigned long long)f;
+            if (g < (unsigned long long)d.csrCap) d.csrCols[g] = o;
             const V3<R> oa0(sA0[0][s], sA0[1][s], sA0[2][s]);
             const V3<R> oa1(sA1[0][s], sA1[1][s], sA1[2][s]);
             bool pen = false;
             R dist;
-            lim = contact_step_limit(d, ks, c, o, oa0, oa1, d.sp[sScene[s]], pen, dist);
+            lim = contact_step_limit(d, ks, g < (unsigned long long)d.relCap ? (size_t)g : NO_STAGE, o, oa0, oa1,
+                                     d.sp[sScene[s]], pen, dist);
             pens += pen;
             dmin = fminf(dmin, (float)dist);
         }
         sLim[t] = lim;
         __syncthreads();
-        const int f0 = max(myOff, base), f1 = min(myOff + nc, base + B);
-        for (int g = f0; g < f1; g++) m = ymin(m, sLim[g - base]);
+        const int f0 = max(myOff, b0), f1 = min(myOff + nc, b0 + B);
+        for (int g = f0; g < f1; g++) m = ymin(m, sLim[g - b0]);
         __syncthreads();
     }
     if (pens) {
@@ -833,6 +888,13 @@ void launch_bvh_refit(const Dev<R>& d, cudaStream_t s) {
 }
 
 template <typename R>
+void launch_lists(const Dev<R>& d, int sortLists, cudaStream_t s) {
+    const int tiles = (d.n + LIST_THREADS - 1) / LIST_THREADS;
+    cudaMemsetAsync(d.listStatus, 0, sizeof(unsigned long long) * (1 + (size_t)tiles), s);
+    k_lists<R><<<tiles, LIST_THREADS, 0, s>>>(d, sortLists);
+}
+
+template <typename R>
 void launch_traverse(const Dev<R>& d, cudaStream_t s) {
     if (d.nseg <= 0) return;
     cudaMemsetAsync(d.numCols, 0, sizeof(int) * d.n, s);
@@ -842,13 +904,13 @@ void launch_traverse(const Dev<R>& d, cudaStream_t s) {
         k_traverse_packet<R><<<blocks, TRAV_THREADS, 0, s>>>(d);
     else
         k_traverse<R><<<blocks, TRAV_THREADS, 0, s>>>(d);
-    k_lists<R><<<(d.nseg + 127) / 128, 128, 0, s>>>(d, 1);
+    launch_lists(d, 1, s);
 }
 
 template <typename R>
 void launch_lists_step_limit(const Dev<R>& d, cudaStream_t s) {
     if (d.nseg <= 0) return;
-    k_lists<R><<<(d.nseg + 127) / 128, 128, 0, s>>>(d, 0);
+    launch_lists(d, 0, s);
 }
 
 template void launch_bvh_rebuild<float>(const Dev<float>&, cudaStream_t, void*, size_t, int);

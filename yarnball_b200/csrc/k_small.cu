@@ -96,7 +96,8 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_small(Dev<R> d, int steps, in
                 const int o = d.cols[col_at(k, c)];
                 bool pen;
                 R dist;
-                const R lim = contact_step_limit(d, k, c, o, a0, a1, sp, pen, dist);
+                const R lim =
+                    contact_step_limit(d, k, c < RELCAP ? rel_at(k, c) : NO_STAGE, o, a0, a1, sp, pen, dist);
                 pens += pen;
                 dmin = fminf(dmin, (float)dist);
                 m = ymin(m, lim);

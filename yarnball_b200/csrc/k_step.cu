@@ -125,29 +125,22 @@ __global__ void __launch_bounds__(NT, MINB) k_iter(Dev<R> d, int src) {
                 Ha.add_diag(dd);
                 Hb.add_diag(dd);
             }
-            // Barrier + friction over this lane's share of the contact list.  Partner
-            // positions relative to p0 are staged per substep for the first RELCAP contacts;
-            // the partner's iterate pair is one 32-byte gather.
+            // Barrier + friction over this lane's share of the contact list (packed slots).
+            // Partner positions relative to p0 are staged per substep in the slots below
+            // relCap; the partner's iterate pair is one 32-byte gather.
             // With PIPE the loads of the lane's next contact are issued before the current
             // contact's arithmetic, so the dependent partner gather overlaps it (more
             // registers); without it each contact loads then computes.
-            const int nc = d.numCols[k];
-            const int* __restrict__ cl = d.cols + col_at(k, 0);
+            unsigned off;
+            const int nc = contact_range(d, k, off);
+            const int* __restrict__ cl = d.csrCols + off;
             const V3<R> e = p1 - p0;
             if constexpr (!PIPE) {
                 for (int c2 = lane; c2 < nc; c2 += T) {
-                    const size_t at = rel_at(k, c2);
                     const int j = __ldg(cl + c2);
+                    if (!partner_ok(d, j)) continue;
                     V3<R> r0, r1;
-                    if (c2 < RELCAP) {
-                        const V4<R> A = d.relA[at];
-                        const R2<R> Bq = d.relB[at];
-                        r0 = V3<R>(A.x, A.y, A.z);
-                        r1 = V3<R>(A.w, Bq.x, Bq.y);
-                    } else {
-                        r0 = xyz(d.pos[j]) - p0;
-                        r1 = xyz(d.pos[j + 1]) - p0;
-                    }
+                    partner_rel(d, off + c2, j, p0, r0, r1);
                     const D2<R> pd = DX[j];
                     contact_term(e, dx, dx1, r0, r1, xyz(pd.a), xyz(pd.b), sp, fa, Ha, fb, Hb);
                 }
@@ -155,39 +148,29 @@ __global__ void __launch_bounds__(NT, MINB) k_iter(Dev<R> d, int src) {
             int c2 = lane;
             V3<R> r0n(R(0)), r1n(R(0));
             D2<R> pdn;
+            bool okn = false;
             if (c2 < nc) {
-                const size_t at = rel_at(k, c2);
                 const int j = __ldg(cl + c2);
-                if (c2 < RELCAP) {
-                    const V4<R> A = d.relA[at];
-                    const R2<R> Bq = d.relB[at];
-                    r0n = V3<R>(A.x, A.y, A.z);
-                    r1n = V3<R>(A.w, Bq.x, Bq.y);
-                } else {
-                    r0n = xyz(d.pos[j]) - p0;
-                    r1n = xyz(d.pos[j + 1]) - p0;
+                okn = partner_ok(d, j);
+                if (okn) {
+                    partner_rel(d, off + c2, j, p0, r0n, r1n);
+                    pdn = DX[j];
                 }
-                pdn = DX[j];
             }
             while (c2 < nc) {
                 const V3<R> r0 = r0n, r1 = r1n;
                 const D2<R> pd = pdn;
+                const bool ok = okn;
                 c2 += T;
                 if (c2 < nc) {
-                    const size_t at = rel_at(k, c2);
                     const int j = __ldg(cl + c2);
-                    if (c2 < RELCAP) {
-                        const V4<R> A = d.relA[at];
-                        const R2<R> Bq = d.relB[at];
-                        r0n = V3<R>(A.x, A.y, A.z);
-                        r1n = V3<R>(A.w, Bq.x, Bq.y);
-                    } else {
-                        r0n = xyz(d.pos[j]) - p0;
-                        r1n = xyz(d.pos[j + 1]) - p0;
+                    okn = partner_ok(d, j);
+                    if (okn) {
+                        partner_rel(d, off + c2, j, p0, r0n, r1n);
+                        pdn = DX[j];
                     }
-                    pdn = DX[j];
                 }
-                contact_term(e, dx, dx1, r0, r1, xyz(pd.a), xyz(pd.b), sp, fa, Ha, fb, Hb);
+                if (ok) contact_term(e, dx, dx1, r0, r1, xyz(pd.a), xyz(pd.b), sp, fa, Ha, fb, Hb);
             }
             }
         }
@@ -269,9 +252,10 @@ __global__ void __launch_bounds__(NT, MINB) k_iter(Dev<R> d, int src) {
 
 // ---------------------------------------------------------------------------------------
 // Load-balanced variant of k_iter (one lane per vertex).  The contact lists of the block's
-// B segments are flattened (block scan of the counts); every thread takes contacts
-// f = tid, tid + B, ... of the flattened list, so a warp never waits for its longest list and
-// the partner gathers of the whole block are in flight together.  Each thread writes its
+// B segments are consecutive in the packed layout (slots base + f, f = 0 .. total - 1); every
+// thread takes contacts f = tid, tid + B, ... of that range, so a warp never waits for its
+// longest list, the partner ids and staged positions are read coalesced, and the partner
+// gathers of the whole block are in flight together.  Each thread writes its
 // contact's 18-value contribution to shared memory (four 16-byte and one 8-byte store); the
 // owning segment then adds its contacts in list order, so the result is deterministic.  The
 // rest (own terms, vertex solve, orientation update) is k_iter's.
@@ -296,6 +280,7 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_bal(Dev<R> d, int src) {
     __shared__ int sOff[B + 1];
     __shared__ int sScene[B];
     __shared__ int sWarp[NW];
+    __shared__ unsigned sBase;
 
     // The contact loop runs first and accumulates from zero; the vertex's own terms (inertia,
     // glue, stretch) are loaded and added after it, so their inputs are not live (in
@@ -304,6 +289,7 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_bal(Dev<R> d, int src) {
     H3<R> Ha, Hb;
     Ha.zero(); Hb.zero();
     int nc = 0, sc = 0;
+    if (t == 0) sBase = d.csrOff[k < 0 ? 0 : k];  // the block's first packed slot (k < n here)
     {
         V3<R> p0(R(0)), e(R(0)), dx(R(0)), dx1(R(0));
         if (valid) {
@@ -320,7 +306,8 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_bal(Dev<R> d, int src) {
             p0 = xyz(d.pos[k]);
             if (fl & F_HAS_NEXT) {
                 e = xyz(d.pos[k + 1]) - p0;
-                nc = d.numCols[k];
+                unsigned off;
+                nc = contact_range(d, k, off);
             }
         }
         sSeg[0][t] = p0.x; sSeg[1][t] = p0.y; sSeg[2][t] = p0.z;
@@ -329,7 +316,7 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_bal(Dev<R> d, int src) {
         sSeg[9][t] = dx1.x; sSeg[10][t] = dx1.y; sSeg[11][t] = dx1.z;
         sScene[t] = sc;
     }
-    // block exclusive scan of the contact counts
+    // block exclusive scan of the contact counts (the block's packed slots are base + offset)
     {
         const int lane = t & 31, w = t >> 5;
         int x = nc;
@@ -346,8 +333,14 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_bal(Dev<R> d, int src) {
         if (t == B - 1) sOff[B] = wo + x;
         __syncthreads();
     }
-    const int total = sOff[B];
-    const int myOff = sOff[t];
+    int total = sOff[B];
+    int myOff = sOff[t];
+    const unsigned base = sBase;
+    if (base > d.csrCap || d.csrCap - base < (unsigned)total) {  // only a packing the list pass reported as failed
+        total = 0;
+        myOff = 0;
+        nc = 0;
+    }
     // Chunks of NT contacts, one per thread.  Each thread writes its own slot index over its
     // contacts of the next chunk before the current chunk's barrier, which publishes it, and
     // the contributions are double buffered: a buffer is written again only after the next
@@ -359,36 +352,23 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_bal(Dev<R> d, int src) {
     // The partner id of this thread's contact is loaded one chunk ahead (after the previous
     // chunk's barrier, before its summation), so a chunk starts with the partner gather.
     int jn = 0;
-    if (t < total) {
-        const int s = sOwn[0][t];
-        jn = __ldg(d.cols + col_at(blockIdx.x * CORE - 1 + s, t - sOff[s]));
-    }
-    for (int base = 0; base < total; base += NT, buf ^= 1) {
-        const int f = base + t;
+    if (t < total) jn = __ldg(d.csrCols + (base + t));
+    for (int b0 = 0; b0 < total; b0 += NT, buf ^= 1) {
+        const int f = b0 + t;
         {
-            const int nb = base + NT;
+            const int nb = b0 + NT;
             const int g1 = min(myOff + nc, nb + NT);
             for (int g = max(myOff, nb); g < g1; g++) sOwn[buf ^ 1][g - nb] = t;
         }
         V3<R> cfa(R(0)), cfb(R(0));
         H3<R> cHa, cHb;
         cHa.zero(); cHb.zero();
-        if (f < total) {
-            const int s = sOwn[buf][t], c = f - sOff[s];
-            const int ks = blockIdx.x * CORE - 1 + s;
-            const size_t at = rel_at(ks, c);
+        if (f < total && partner_ok(d, jn)) {
+            const int s = sOwn[buf][t];
             const int j = jn;
             const V3<R> sp0(sSeg[0][s], sSeg[1][s], sSeg[2][s]);
             V3<R> r0, r1;
-            if (c < RELCAP) {
-                const V4<R> A = d.relA[at];
-                const R2<R> Bq = d.relB[at];
-                r0 = V3<R>(A.x, A.y, A.z);
-                r1 = V3<R>(A.w, Bq.x, Bq.y);
-            } else {
-                r0 = xyz(d.pos[j]) - sp0;
-                r1 = xyz(d.pos[j + 1]) - sp0;
-            }
+            partner_rel(d, base + f, j, sp0, r0, r1);
             const D2<R> pd = DX[j];
             const V3<R> se(sSeg[3][s], sSeg[4][s], sSeg[5][s]);
             const V3<R> sdx(sSeg[6][s], sSeg[7][s], sSeg[8][s]);
@@ -408,20 +388,19 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_bal(Dev<R> d, int src) {
         __syncthreads();
         {
             // next chunk: partner id, and the staged partner positions into L1
-            const int fn = base + NT + t;
+            const int fn = b0 + NT + t;
             if (fn < total) {
-                const int s = sOwn[buf ^ 1][t], c = fn - sOff[s];
-                const int ks = blockIdx.x * CORE - 1 + s;
-                jn = __ldg(d.cols + col_at(ks, c));
-                if (c < RELCAP) {
-                    prefetch_l1(d.relA + rel_at(ks, c));
-                    prefetch_l1(d.relB + rel_at(ks, c));
+                const unsigned g = base + fn;
+                jn = __ldg(d.csrCols + g);
+                if (g < d.relCap) {
+                    prefetch_l1(d.relA + g);
+                    prefetch_l1(d.relB + g);
                 }
             }
         }
-        const int f0 = max(myOff, base), f1 = min(myOff + nc, base + NT);
+        const int f0 = max(myOff, b0), f1 = min(myOff + nc, b0 + NT);
         for (int g = f0; g < f1; g++) {
-            const int i = g - base;
+            const int i = g - b0;
             const V4<R> w0 = sCon4[buf][0][i], w1 = sCon4[buf][1][i], w2 = sCon4[buf][2][i], w3 = sCon4[buf][3][i];
             const R2<R> w4 = sCon2[buf][i];
             fa += V3<R>(w0.x, w0.y, w0.z);
@@ -517,6 +496,7 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_wbal(Dev<R> d, int src) {
     __shared__ R sCon[18][B];  // contributions of one chunk of contacts
     __shared__ int sOffW[NW][33];
     __shared__ int sScene[B];
+    __shared__ unsigned sKOff[B];  // first packed slot of each slot's contacts
 
     // The contact loop runs first and accumulates from zero; the vertex's own terms are
     // loaded and added after it (their inputs are not live across the loop).
@@ -524,6 +504,7 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_wbal(Dev<R> d, int src) {
     H3<R> Ha, Hb;
     Ha.zero(); Hb.zero();
     int nc = 0, sc = 0;
+    unsigned kOff = 0;
     {
         V3<R> p0(R(0)), e(R(0)), dx(R(0)), dx1(R(0));
         if (valid) {
@@ -535,7 +516,7 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_wbal(Dev<R> d, int src) {
             p0 = xyz(d.pos[k]);
             if (fl & F_HAS_NEXT) {
                 e = xyz(d.pos[k + 1]) - p0;
-                nc = d.numCols[k];
+                nc = contact_range(d, k, kOff);
             }
         }
         sSeg[0][t] = p0.x; sSeg[1][t] = p0.y; sSeg[2][t] = p0.z;
@@ -543,6 +524,7 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_wbal(Dev<R> d, int src) {
         sSeg[6][t] = dx.x; sSeg[7][t] = dx.y; sSeg[8][t] = dx.z;
         sSeg[9][t] = dx1.x; sSeg[10][t] = dx1.y; sSeg[11][t] = dx1.z;
         sScene[t] = sc;
+        sKOff[t] = kOff;
     }
     // warp exclusive scan of the contact counts: each warp flattens its own 32 vertices
     const int lane = t & 31, wp = t >> 5, w0 = wp << 5;
@@ -569,25 +551,18 @@ __global__ void __launch_bounds__(NT, MINB) k_iter_wbal(Dev<R> d, int src) {
                 if (sOffW[wp][mid] <= f) lo = mid; else hi = mid - 1;
             }
             const int s = w0 + lo, c = f - sOffW[wp][lo];
-            const int ks = blockIdx.x * CORE - 1 + s;
-            const size_t at = rel_at(ks, c);
-            const int j = __ldg(d.cols + col_at(ks, c));
-            const V3<R> sp0(sSeg[0][s], sSeg[1][s], sSeg[2][s]);
-            V3<R> r0, r1;
-            if (c < RELCAP) {
-                const V4<R> A = d.relA[at];
-                const R2<R> Bq = d.relB[at];
-                r0 = V3<R>(A.x, A.y, A.z);
-                r1 = V3<R>(A.w, Bq.x, Bq.y);
-            } else {
-                r0 = xyz(d.pos[j]) - sp0;
-                r1 = xyz(d.pos[j + 1]) - sp0;
+            const unsigned g = sKOff[s] + c;
+            const int j = __ldg(d.csrCols + g);
+            if (partner_ok(d, j)) {
+                const V3<R> sp0(sSeg[0][s], sSeg[1][s], sSeg[2][s]);
+                V3<R> r0, r1;
+                partner_rel(d, g, j, sp0, r0, r1);
+                const D2<R> pd = DX[j];
+                const V3<R> se(sSeg[3][s], sSeg[4][s], sSeg[5][s]);
+                const V3<R> sdx(sSeg[6][s], sSeg[7][s], sSeg[8][s]);
+                const V3<R> sdx1(sSeg[9][s], sSeg[10][s], sSeg[11][s]);
+                contact_term(se, sdx, sdx1, r0, r1, xyz(pd.a), xyz(pd.b), d.sp[sScene[s]], cfa, cHa, cfb, cHb);
             }
-            const D2<R> pd = DX[j];
-            const V3<R> se(sSeg[3][s], sSeg[4][s], sSeg[5][s]);
-            const V3<R> sdx(sSeg[6][s], sSeg[7][s], sSeg[8][s]);
-            const V3<R> sdx1(sSeg[9][s], sSeg[10][s], sSeg[11][s]);
-            contact_term(se, sdx, sdx1, r0, r1, xyz(pd.a), xyz(pd.b), d.sp[sScene[s]], cfa, cHa, cfb, cHb);
         }
         sCon[0][t] = cfa.x; sCon[1][t] = cfa.y; sCon[2][t] = cfa.z;
         sCon[3][t] = cfb.x; sCon[4][t] = cfb.y; sCon[5][t] = cfb.z;

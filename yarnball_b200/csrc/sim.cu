@@ -349,6 +349,12 @@ struct Engine : EngineBase {
         want((void**)&d.cols, sizeof(int) * n * MAX_COLS);
         want((void**)&d.relA, sizeof(V4<R>) * n * RELCAP);
         want((void**)&d.relB, sizeof(R2<R>) * n * RELCAP);
+        // packed contacts: every list at its cap fits (slot indices are 32-bit)
+        const size_t csrCap = std::min(n * (size_t)MAX_COLS, (size_t)0xffffffffu);
+        const size_t listTiles = (n + LIST_THREADS - 1) / LIST_THREADS;
+        want((void**)&d.csrOff, sizeof(unsigned) * (n + 1));
+        want((void**)&d.csrCols, sizeof(int) * csrCap);
+        want((void**)&d.listStatus, sizeof(unsigned long long) * (1 + listTiles));
         want((void**)&d.segs, sizeof(int) * n);
         want((void**)&spDev, sizeof(SceneParams<R>) * ns);
         want((void**)&d.err, sizeof(int) * EW_COUNT);
@@ -390,6 +396,8 @@ struct Engine : EngineBase {
         d.numScenes = S->numScenes;
         d.nseg = 0;
         d.sp = spDev;
+        d.csrCap = (unsigned)csrCap;
+        d.relCap = (unsigned)(n * RELCAP);
         {
             int dev = 0, sms = 148;
             cudaGetDevice(&dev);
@@ -403,6 +411,8 @@ struct Engine : EngineBase {
         static const int kInfBits = 0x7f800000;  // EW_MIN_DIST starts at +inf
         YB_CUDA(cudaMemcpyAsync(d.err + EW_MIN_DIST, &kInfBits, sizeof(int), cudaMemcpyHostToDevice, S->stream));
         YB_CUDA(cudaMemsetAsync(d.numCols, 0, sizeof(int) * n, S->stream));
+        // no packed contacts until the first list pass (a Newton launch before it reads none)
+        YB_CUDA(cudaMemsetAsync(d.csrOff, 0, sizeof(unsigned) * (n + 1), S->stream));
         YB_CUDA(cudaMemsetAsync(d.lastVel, 0, sizeof(V4<R>) * n, S->stream));
         YB_CUDA(cudaMemsetAsync(d.refitCount, 0, sizeof(unsigned) * nn, S->stream));
         // records never built read as empty (last = 0 prunes every entry); until the first

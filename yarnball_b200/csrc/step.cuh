@@ -107,6 +107,38 @@ __device__ __forceinline__ void contact_term(V3<R> e, V3<R> dx0, V3<R> dx1, V3<R
     }
 }
 
+// Packed contacts of segment k (written by the list pass of this substep): first slot in off,
+// count returned.  A range the packed arrays cannot hold (the list pass reports it) reads as
+// empty.
+template <typename R>
+__device__ __forceinline__ int contact_range(const Dev<R>& d, int k, unsigned& off) {
+    off = d.csrOff[k];
+    const unsigned end = d.csrOff[k + 1];
+    if (end < off || end - off > (unsigned)MAX_COLS || end > d.csrCap) return 0;
+    return (int)(end - off);
+}
+
+// Whether j can be a contact partner (a segment start: j and j + 1 are vertices).
+template <typename R>
+__device__ __forceinline__ bool partner_ok(const Dev<R>& d, int j) {
+    return (unsigned)j < (unsigned)(d.n - 1);
+}
+
+// Endpoints of partner segment j relative to p0: staged by the list pass in packed slot g, or
+// gathered when g is past the staging capacity (the same differences either way).
+template <typename R>
+__device__ __forceinline__ void partner_rel(const Dev<R>& d, unsigned g, int j, const V3<R>& p0, V3<R>& r0, V3<R>& r1) {
+    if (g < d.relCap) {
+        const V4<R> A = d.relA[g];
+        const R2<R> Bq = d.relB[g];
+        r0 = V3<R>(A.x, A.y, A.z);
+        r1 = V3<R>(A.w, Bq.x, Bq.y);
+    } else {
+        r0 = xyz(d.pos[j]) - p0;
+        r1 = xyz(d.pos[j + 1]) - p0;
+    }
+}
+
 // Predicted iterate pair of vertex i (dx[i], dx[i+1]) into dx[0] (the k_init pass).
 template <typename R>
 __device__ __forceinline__ void init_vertex(const Dev<R>& d, int i) {

@@ -5,11 +5,14 @@ scene that asks for a number of frames of 1/30 s.  The server keeps every admitt
 state on the device between frames and advances all of them with one batched advance() per
 frame, so requests of different sizes share every kernel launch:
 
-  * a request waits in a FIFO queue; host threads set the head of the queue up (geometry,
-    configure, upload) as one-scene Sims while the frames run, a bounded number of vertices
-    ahead, so set-up overlaps device work;
-  * a set-up request is admitted at the next frame boundary if the device-memory budget (the
-    staged Sims and two batch allocations) and the optional per-frame vertex cap allow;
+  * a request waits in a FIFO queue; host threads generate the geometry of the head of the
+    queue while the frames run, a bounded number of vertices ahead, so that host work overlaps
+    device work;
+  * a request whose geometry is ready is admitted at the next frame boundary if the
+    device-memory budget (two batch allocations) and the optional per-frame vertex cap allow;
+    the frame thread then builds it as a one-scene Sim (configure, upload): every CUDA call of
+    the server is made by the frame thread, so no allocation or release of another thread can
+    meet a graph capture or a frame in flight;
   * when membership changes, the batch is rebuilt by copying every remaining and newly
     admitted scene device to device (yb_batch_gather), reusing the previous batch's
     allocation when it is large enough (two allocations alternate);
@@ -23,7 +26,6 @@ the multi-block kernels to rounding.
 """
 import collections
 import math
-import threading
 from concurrent.futures import Future, ThreadPoolExecutor
 
 import numpy as np
@@ -43,18 +45,11 @@ class Request:
         self.seed = seed
         self.done_frames = 0
         self.staging = None           # one-scene Sim until admitted
-        self.future = None            # its set-up on a host thread
+        self.future = None            # its geometry, generated on a host thread
         self.admitted_at = None
         self.finished_at = None
         self.result = None            # (positions, velocities, rotors) after the last frame
         self.vertices = int(np.sum(spec[0]))
-
-
-# Device work of the set-up threads (allocation, configure, upload, release) and the frame
-# thread's batch work (gather, advance with its graph capture, download) never overlap: a
-# stream capture must not see another thread's allocation or release, which may synchronise
-# the device.  The host part of a set-up (the geometry) runs outside the lock, beside frames.
-_device_lock = threading.Lock()
 
 
 def request_geometry(req):
@@ -98,12 +93,11 @@ class Server:
     """Continuous batching on one GPU.
 
     budget_bytes        device memory for the batch (two allocations, gathered alternately)
-                        and the requests staged ahead of admission
     max_batch_vertices  optional cap on the vertices advanced per frame: it bounds the frame
                         latency (a frame's time grows with the batch) at the price of queueing
-    setup_threads       host threads that set requests up (geometry, configure, upload) ahead
-                        of admission, while frames run; 0 sets them up on the frame thread
-    prefetch_vertices   how many vertices of queued requests may be staged ahead
+    setup_threads       host threads that generate request geometry ahead of admission, while
+                        frames run; 0 generates it on the frame thread
+    prefetch_vertices   how many vertices of queued requests may have geometry staged ahead
     """
 
     def __init__(self, budget_bytes=120e9, shape=(128, 0), bytes_per_vertex=None, capacity_headroom=1.25,
@@ -135,9 +129,14 @@ class Server:
     def _staged_vertices(self):
         return sum(r.vertices for r in self.queue if r.future is not None)
 
+    def _build(self, r):
+        """The admitted request as a one-scene Sim (frame thread)."""
+        return build_request_sim(r, self.shape, pos=r.future.result())
+
     # ---- request flow ---------------------------------------------------------------
     def submit(self, req):
-        """Queues a request; its set-up starts on a host thread when the prefetch window allows."""
+        """Queues a request; its geometry is generated on a host thread when the prefetch window
+        allows."""
         req.future = None
         self.queue.append(req)
         self._stage()
@@ -151,50 +150,40 @@ class Server:
                 break
             if self.pool is None:
                 f = Future()
-                f.set_result(build_request_sim(r, self.shape))
+                f.set_result(request_geometry(r))
                 r.future = f
             else:
-                r.future = self.pool.submit(self._set_up, r)
+                r.future = self.pool.submit(request_geometry, r)
             staged += r.vertices
-
-    def _set_up(self, r):
-        pos = request_geometry(r)  # host work, beside the frames
-        with _device_lock:
-            return build_request_sim(r, self.shape, pos=pos)
 
     def _admit(self):
         joined = []
         verts = sum(r.vertices for r in self.active)
+        joinedVerts = 0
         while self.queue:
             r = self.queue[0]
             if r.future is None:
                 break
             if not r.future.done():
-                break  # not set up yet: the batch goes on without it
-            sim = r.future.result()
-            self._bytes_per_vertex(sim)
-            if self.active or joined:
-                # two batch allocations of the grown size must fit the budget with the staged scenes
-                need = (2 * self.headroom * (verts + r.vertices) + self._staged_vertices()) * self.bpv
+                break  # geometry not ready: the batch goes on without it
+            if (self.active or joined) and self.bpv is not None:
+                # two batch allocations of the grown size and the one-scene Sims of this frame's
+                # admissions (released after the gather) must fit the budget
+                need = (2 * self.headroom * (verts + r.vertices) + joinedVerts + r.vertices) * self.bpv
                 if need > self.budget or (self.max_batch and verts + r.vertices > self.max_batch):
                     break
+            sim = self._build(r)
+            self._bytes_per_vertex(sim)
             self.queue.popleft()
             r.staging = sim
             joined.append(r)
             verts += r.vertices
+            joinedVerts += r.vertices
         self._stage()
         return joined
 
     def _close_later(self, sim):
-        if self.pool is None:
-            sim.close()
-        else:
-            self.pool.submit(self._release, sim)
-
-    @staticmethod
-    def _release(sim):
-        with _device_lock:
-            sim.close()
+        sim.close()
 
     def _regather(self, keep, joined):
         sources = [(self.batch, i) for i in keep] + [(r.staging, 0) for r in joined]
@@ -223,11 +212,7 @@ class Server:
         """One frame boundary: retire, admit (unless admit is False), re-gather if needed,
         advance one frame."""
         if admit and not self.active and self.queue and self.queue[0].future is not None:
-            self.queue[0].future.result()  # an idle server waits for its next request (unlocked)
-        with _device_lock:
-            return self._step(now, admit)
-
-    def _step(self, now, admit):
+            self.queue[0].future.result()  # an idle server waits for its next request
         self.queue_lengths.append(len(self.queue))
         keep = [i for i, r in enumerate(self.active) if r.done_frames < r.frames]
         joined = self._admit() if admit else []
@@ -271,9 +256,6 @@ class Server:
         for b in (self.batch, self.spare):
             if b is not None:
                 b.close()
-        for r in self.queue:
-            if r.future is not None:
-                r.future.result().close()
         self.batch = self.spare = None
 
 
