@@ -326,12 +326,15 @@ def run_ours(args):
     peak, peak_kind = load_peaks()
     tr = load_traffic()
     traffic, traffic_src = None, None
-    if tr and tr.get("vertices") == n:
-        traffic = tr["dram_bytes_per_launch"]  # captured on this very workload
-        traffic_src = "ncu capture of one launch of this workload (%s)" % tr["summary"]
+    if tr and tr.get("vertices") == n and tr.get("warmup") == args.warmup:
+        traffic = tr["dram_bytes_per_launch"]  # captured on this very workload and state
+        traffic_src = "ncu capture of one launch of this workload after %d warm-up frames (%s)" % (
+            tr["warmup"], tr["summary"])
     elif tr:
-        traffic = tr["dram_bytes_per_vertex"] * n
-        traffic_src = "ncu capture at %d vertices scaled by the vertex count (%s)" % (tr["vertices"], tr["summary"])
+        # another state or size: the captured traffic per algorithmic byte
+        traffic = tr["dram_bytes_per_launch"] * bytes_per_launch / tr["algorithmic_bytes_per_launch"]
+        traffic_src = "ncu capture (%d vertices, %d warm-up frames, c = %.2f) scaled by the algorithmic bytes (%s)" % (
+            tr["vertices"], tr["warmup"], tr["cbar_at_capture"], tr["summary"])
     prof_total = sum(prof_ms.values())
     roofline = {
         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

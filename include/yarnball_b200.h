@@ -197,7 +197,9 @@ yb_status yb_get_tuning(yb_sim* sim, int32_t* iterThreads, int32_t* lanesPerVert
 yb_status yb_autotune(yb_sim* sim, int32_t* bestThreads, int32_t* bestLanes, int32_t* bestPipelined,
                       float* bestMs);
 
-/* Broadphase walk of the BVH: packet = 1 (default) walks the tree once per warp for 32
+/* Broadphase walk of the BVH: packet = 2 (default) walks the tree once per query with the
+ * warp's node records loaded cooperatively (whole 128-byte lines per load, through shared
+ * memory; in the FP64 build each lane loads its own), packet = 1 once per warp for 32
  * consecutive queries, packet = 0 once per query.  The contact lists are identical. */
 yb_status yb_set_traversal(yb_sim* sim, int32_t packet);
 yb_status yb_get_traversal(yb_sim* sim, int32_t* packet);

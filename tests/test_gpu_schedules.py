@@ -259,15 +259,16 @@ def test_diagnostics_vs_oracle_fp64_evaluation():
 
 @pytest.mark.parametrize("which", ["pile", "batch"])
 def test_packet_and_per_query_traversal_give_the_same_lists(which):
-    """The broadphase walk per warp of 32 queries (the default) and per query keep the same
-    pairs, on a rebuilt and on a refitted tree; both equal the oracle's."""
+    """The three broadphase walks (per warp of 32 queries, the default; per query; per query
+    with the warp's node records loaded cooperatively) keep the same pairs, on a rebuilt and on
+    a refitted tree; all equal the oracle's."""
     if which == "pile":
         build = lambda: scenes.build_pile(seed=1)  # noqa: E731  (the full 262,144-vertex pile)
     else:
         spec = scenes.batched_spec(seed=7, num_scenes=24, cap=1500000)
         build = lambda: scenes.build_batched(seed=7, spec=spec)[0]  # noqa: E731
     out = {}
-    for packet in (True, False):
+    for packet in (1, 0, 2):
         sim = build()
         sim.set_traversal(packet)
         sim.advance(FRAME)
@@ -280,4 +281,4 @@ def test_packet_and_per_query_traversal_give_the_same_lists(which):
         _compare_lists(sim, orc)
         sim.close()
         orc.close()
-    assert np.array_equal(out[True][0], out[False][0])
+    assert np.array_equal(out[1][0], out[0][0]) and np.array_equal(out[1][0], out[2][0])

@@ -178,12 +178,18 @@ struct Dev {
     int* sceneRoot;   // child code of each scene's subtree root (or INT_MIN when empty)
     int* sceneLast;   // sorted position of the last leaf of each scene's subtree
     unsigned* travNext;   // next query (sorted position) handed out by the traversal
-    int travBlocks;       // persistent traversal grid
-    int travPacket;       // 1: one walk per warp for 32 queries (k_traverse_packet), 0: one per lane
+    int travBlocks[3];    // persistent traversal grid of each walk mode (travPacket)
+    int travPacket;       // 2: one walk per lane with warp-cooperative record loads (default),
+                          // 1: one walk per warp for 32 queries (k_traverse_packet), 0: one per lane
     unsigned long long* keys[2];
     int* vals[2];
     unsigned* sceneBox;   // 6 ordered-uint per scene: min xyz, max xyz of segment midpoints
 };
+
+// Hint: bring the line holding p into L1 (no register is held until the data is used).
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
 
 // --- kernel launchers (stream-ordered; no host synchronisation) ---
 template <typename R> void launch_init(const Dev<R>& d, cudaStream_t s);
@@ -192,7 +198,7 @@ template <typename R> void launch_iter(const Dev<R>& d, int srcBuf, int threads,
 template <typename R> void launch_bvh_rebuild(const Dev<R>& d, cudaStream_t s, void* sortScratch, size_t sortScratchBytes, int keyBits);
 template <typename R> void launch_bvh_refit(const Dev<R>& d, cudaStream_t s);
 template <typename R> void launch_traverse(const Dev<R>& d, cudaStream_t s);  // + list sort + step limit (2 kernels)
-template <typename R> int traverse_blocks_per_sm();  // resident traversal blocks per SM (persistent grid)
+template <typename R> int traverse_blocks_per_sm(int mode);  // resident traversal blocks per SM (persistent grid)
 template <typename R> void launch_lists_step_limit(const Dev<R>& d, cudaStream_t s);  // step limit over segments
 template <typename R> void launch_bvh_reset(const Dev<R>& d, cudaStream_t s);
 // Places driven vertices on their prescribed motion at the start of an advance of length dt.

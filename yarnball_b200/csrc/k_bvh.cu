@@ -350,10 +350,34 @@ __device__ __forceinline__ void trav_load_wide(const WNode<R>* wide, int node, W
     }
 }
 
-template <typename R>
+// Warp-cooperative load of the 32 lanes' current records (FP32 records: eight 16-byte
+// pieces, one 128-byte line).  Loading its own record, each lane would touch 32 different lines
+// with each of its 8 loads (256 L1 wavefronts per step of the warp); here load r fetches piece
+// (lane & 7) of the record of lane 4r + (lane >> 3), so each load covers 4 whole lines (32
+// wavefronts per step), and the pieces reach their lanes through shared memory (rows padded to
+// 9 pieces, so the reads back are free of bank conflicts).  node < 0: the lane loads nothing.
+constexpr int COOP_ROW = 9;
+
+__device__ __forceinline__ void coop_load_wide(const WNode<float>* wide, int node, float4 (*rows)[COOP_ROW], int lane,
+                                               WNode<float>& w) {
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+        const int owner = 4 * r + (lane >> 3);
+        const int on = __shfl_sync(0xffffffffu, node, owner);
+        if (on >= 0) rows[owner][lane & 7] = __ldg(reinterpret_cast<const float4*>(wide + on) + (lane & 7));
+    }
+    __syncwarp();
+    float4* dst = reinterpret_cast<float4*>(&w);
+#pragma unroll
+    for (int k = 0; k < 8; k++) dst[k] = rows[lane][k];
+    __syncwarp();
+}
+
+template <typename R, bool COOP>
 __global__ void __launch_bounds__(TRAV_THREADS) k_traverse(Dev<R> d) {
     __shared__ int sQx[TRAV_WARPS][TRAV_QCAP];
     __shared__ int sQy[TRAV_WARPS][TRAV_QCAP];
+    __shared__ float4 sRec[COOP ? TRAV_WARPS : 1][COOP ? 32 : 1][COOP_ROW];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     const int nseg = d.nseg;
@@ -406,9 +430,10 @@ __global__ void __launch_bounds__(TRAV_THREADS) k_traverse(Dev<R> d) {
             atomicOr(&d.err[EW_INTERNAL], IE_BVH_STACK);
             walking = false;
         }
+        WNode<R> w;
+        if constexpr (COOP && sizeof(R) == 4) coop_load_wide(d.wide, walking ? node : -1, sRec[warp], lane, w);
         if (walking) {
-            WNode<R> w;
-            trav_load_wide(d.wide, node, w);
+            if constexpr (!(COOP && sizeof(R) == 4)) trav_load_wide(d.wide, node, w);
             int next = -1;
 #pragma unroll
             for (int e = 0; e < 4; e++) {
@@ -899,11 +924,13 @@ void launch_traverse(const Dev<R>& d, cudaStream_t s) {
     if (d.nseg <= 0) return;
     cudaMemsetAsync(d.numCols, 0, sizeof(int) * d.n, s);
     cudaMemsetAsync(d.travNext, 0, sizeof(unsigned), s);
-    const int blocks = min((d.nseg + TRAV_THREADS - 1) / TRAV_THREADS, max(d.travBlocks, 1));
-    if (d.travPacket)
+    const int blocks = min((d.nseg + TRAV_THREADS - 1) / TRAV_THREADS, max(d.travBlocks[d.travPacket], 1));
+    if (d.travPacket == 1)
         k_traverse_packet<R><<<blocks, TRAV_THREADS, 0, s>>>(d);
+    else if (d.travPacket == 2)
+        k_traverse<R, true><<<blocks, TRAV_THREADS, 0, s>>>(d);
     else
-        k_traverse<R><<<blocks, TRAV_THREADS, 0, s>>>(d);
+        k_traverse<R, false><<<blocks, TRAV_THREADS, 0, s>>>(d);
     launch_lists(d, 1, s);
 }
 
@@ -920,18 +947,20 @@ template void launch_bvh_refit<double>(const Dev<double>&, cudaStream_t);
 template void launch_bvh_reset<float>(const Dev<float>&, cudaStream_t);
 template void launch_bvh_reset<double>(const Dev<double>&, cudaStream_t);
 template <typename R>
-int traverse_blocks_per_sm() {  // resident blocks of both traversal kernels (the smaller)
-    int b = 0, c = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_traverse<R>, TRAV_THREADS, 0) != cudaSuccess || b < 1 ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_traverse_packet<R>, TRAV_THREADS, 0) != cudaSuccess ||
-        c < 1) {
+int traverse_blocks_per_sm(int mode) {  // resident blocks of the traversal kernel of a walk mode
+    int b = 0;
+    const cudaError_t e =
+        mode == 1 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_traverse_packet<R>, TRAV_THREADS, 0)
+        : mode == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_traverse<R, true>, TRAV_THREADS, 0)
+                    : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_traverse<R, false>, TRAV_THREADS, 0);
+    if (e != cudaSuccess || b < 1) {
         cudaGetLastError();
         return 4;
     }
-    return b < c ? b : c;
+    return b;
 }
-template int traverse_blocks_per_sm<float>();
-template int traverse_blocks_per_sm<double>();
+template int traverse_blocks_per_sm<float>(int);
+template int traverse_blocks_per_sm<double>(int);
 template void launch_traverse<float>(const Dev<float>&, cudaStream_t);
 template void launch_lists_step_limit<float>(const Dev<float>&, cudaStream_t);
 template void launch_lists_step_limit<double>(const Dev<double>&, cudaStream_t);

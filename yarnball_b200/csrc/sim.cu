@@ -94,7 +94,7 @@ struct yb_sim {
     int iterLanes = 0;
     int iterPipe = 0;
     int useGraphs = 1;
-    int travPacket = 1;  // broadphase walk: 1 per warp of 32 queries, 0 per query
+    int travPacket = 2;  // broadphase walk: 2 per query with cooperative loads, 1 per warp of 32 queries, 0 per query
     int useSmall = 1;    // advance small simulations with the one-block kernel
     uint64_t launches = 0;
     cudaStream_t stream = nullptr;     // active stream (own or the caller's)
@@ -402,7 +402,7 @@ struct Engine : EngineBase {
             int dev = 0, sms = 148;
             cudaGetDevice(&dev);
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            d.travBlocks = sms * traverse_blocks_per_sm<R>();
+            for (int m = 0; m < 3; m++) d.travBlocks[m] = sms * traverse_blocks_per_sm<R>(m);
         }
         d.travPacket = S->travPacket;
         YB_CUDA(cudaHostAlloc((void**)&spHost, sizeof(SceneParams<R>) * ns, cudaHostAllocDefault));
@@ -1485,7 +1485,7 @@ yb_status yb_set_small_path(yb_sim* S, int32_t enable) {
 }
 
 yb_status yb_set_traversal(yb_sim* S, int32_t packet) {
-    if (!S || (packet != 0 && packet != 1)) return YB_ERR_INVALID_ARGUMENT;
+    if (!S || packet < 0 || packet > 2) return YB_ERR_INVALID_ARGUMENT;
     S->travPacket = packet;
     if (S->eng) S->eng->set_traversal(packet);
     return YB_OK;

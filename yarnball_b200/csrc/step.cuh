@@ -47,10 +47,6 @@ __device__ __forceinline__ V3<R> predict(const Dev<R>& d, int i) {
 // IPC log barrier E(d) = -kCollision (d-1)^2 ln d on the normalised gap d, clamped to 1e-3:
 // returns dH = E''(d) / b^2 and the force magnitude ff (cosserat.cu:114-125).  Below d=1e-2
 // the log and the reciprocals are evaluated in FP64.
-// Hint: bring the line holding p into L1 (no register is held until the data is used).
-__device__ __forceinline__ void prefetch_l1(const void* p) {
-    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
-}
 
 template <typename R>
 __device__ __forceinline__ void barrier_terms(R d, R kCol, R invb, R& dH, R& ff) {

@@ -386,9 +386,11 @@ class Sim:
         per advance)."""
         check(self._lib.yb_set_small_path(self._h, 1 if enable else 0), "small path")
 
-    def set_traversal(self, packet=True):
-        """Broadphase walk: one per warp of 32 queries (packet) or one per query."""
-        check(self._lib.yb_set_traversal(self._h, 1 if packet else 0), "traversal")
+    def set_traversal(self, mode=2):
+        """Broadphase walk: 2 (default) one per query with the warp's node records loaded
+        cooperatively, True / 1 one per warp of 32 queries (packet), False / 0 one per query."""
+        m = (1 if mode else 0) if isinstance(mode, bool) else int(mode)
+        check(self._lib.yb_set_traversal(self._h, m), "traversal")
 
     def debug_last_vel(self):
         lv = np.zeros((self.numVerts, 3))
