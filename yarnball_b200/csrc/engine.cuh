@@ -122,12 +122,16 @@ struct alignas(16) BNode {         // internal BVH node: boxes of both children 
 // 4-wide view of the binary tree for traversal: entry e of node i is a grandchild of binary
 // node i (or a child, when that child is a leaf), with its box, child code and the sorted
 // position of the last leaf below it.  Unused entries have code WIDE_NONE and an empty box.
+// An entry is contiguous (32 bytes in FP32), so a walk can read one entry at a time.
 constexpr int WIDE_NONE = -2147483647 - 1;
 template <typename R>
+struct WEntry {
+    R mn[3], mx[3];
+    int code, last;
+};
+template <typename R>
 struct alignas(16) WNode {
-    R mn[3][4], mx[3][4];
-    int code[4];
-    int last[4];
+    WEntry<R> e[4];
 };
 
 // Query record of a sorted leaf, written by the refit for the traversal: the segment's padded

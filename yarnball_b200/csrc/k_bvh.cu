@@ -284,11 +284,11 @@ __global__ void __launch_bounds__(256) k_widen(Dev<R> d) {
     auto put = [&](int code, const R* mn, const R* mx, int last) {
 #pragma unroll
         for (int a = 0; a < 3; a++) {
-            w.mn[a][e] = mn[a];
-            w.mx[a][e] = mx[a];
+            w.e[e].mn[a] = mn[a];
+            w.e[e].mx[a] = mx[a];
         }
-        w.code[e] = code;
-        w.last[e] = last;
+        w.e[e].code = code;
+        w.e[e].last = last;
         e++;
     };
     const int lastI = d.nodeLast[i];
@@ -358,8 +358,7 @@ __device__ __forceinline__ void trav_load_wide(const WNode<R>* wide, int node, W
 // 9 pieces, so the reads back are free of bank conflicts).  node < 0: the lane loads nothing.
 constexpr int COOP_ROW = 9;
 
-__device__ __forceinline__ void coop_load_wide(const WNode<float>* wide, int node, float4 (*rows)[COOP_ROW], int lane,
-                                               WNode<float>& w) {
+__device__ __forceinline__ void coop_load_wide(const WNode<float>* wide, int node, float4 (*rows)[COOP_ROW], int lane) {
 #pragma unroll
     for (int r = 0; r < 8; r++) {
         const int owner = 4 * r + (lane >> 3);
@@ -367,10 +366,24 @@ __device__ __forceinline__ void coop_load_wide(const WNode<float>* wide, int nod
         if (on >= 0) rows[owner][lane & 7] = __ldg(reinterpret_cast<const float4*>(wide + on) + (lane & 7));
     }
     __syncwarp();
-    float4* dst = reinterpret_cast<float4*>(&w);
-#pragma unroll
-    for (int k = 0; k < 8; k++) dst[k] = rows[lane][k];
-    __syncwarp();
+}
+
+// Entry e of a wide record: from the lane's shared-memory row (cooperative load) or from
+// the record in registers.
+template <typename R>
+__device__ __forceinline__ WEntry<R> wide_entry(const WNode<R>& w, const float4* row, int e, bool fromRow) {
+    if constexpr (sizeof(R) == 4) {
+        if (fromRow) {
+            const float4 A = row[2 * e], B = row[2 * e + 1];  // (mn xyz, mx x), (mx yz, code, last)
+            WEntry<R> x;
+            x.mn[0] = A.x; x.mn[1] = A.y; x.mn[2] = A.z;
+            x.mx[0] = A.w; x.mx[1] = B.x; x.mx[2] = B.y;
+            x.code = __float_as_int(B.z);
+            x.last = __float_as_int(B.w);
+            return x;
+        }
+    }
+    return w.e[e];
 }
 
 template <typename R, bool COOP>
@@ -430,18 +443,19 @@ __global__ void __launch_bounds__(TRAV_THREADS) k_traverse(Dev<R> d) {
             atomicOr(&d.err[EW_INTERNAL], IE_BVH_STACK);
             walking = false;
         }
+        constexpr bool ROW = COOP && sizeof(R) == 4;
         WNode<R> w;
-        if constexpr (COOP && sizeof(R) == 4) coop_load_wide(d.wide, walking ? node : -1, sRec[warp], lane, w);
+        if constexpr (ROW) coop_load_wide(d.wide, walking ? node : -1, sRec[warp], lane);
         if (walking) {
-            if constexpr (!(COOP && sizeof(R) == 4)) trav_load_wide(d.wide, node, w);
+            if constexpr (!ROW) trav_load_wide(d.wide, node, w);
             int next = -1;
 #pragma unroll
             for (int e = 0; e < 4; e++) {
-                const bool hit = w.last[e] > qi && qb.mn[0] <= w.mx[0][e] && w.mn[0][e] <= qb.mx[0] &&
-                                 qb.mn[1] <= w.mx[1][e] && w.mn[1][e] <= qb.mx[1] && qb.mn[2] <= w.mx[2][e] &&
-                                 w.mn[2][e] <= qb.mx[2];
+                const WEntry<R> x = wide_entry(w, sRec[COOP ? warp : 0][COOP ? lane : 0], e, ROW);
+                const bool hit = x.last > qi && qb.mn[0] <= x.mx[0] && x.mn[0] <= qb.mx[0] && qb.mn[1] <= x.mx[1] &&
+                                 x.mn[1] <= qb.mx[1] && qb.mn[2] <= x.mx[2] && x.mn[2] <= qb.mx[2];
                 if (!hit) continue;
-                const int c = w.code[e];
+                const int c = x.code;
                 if (c < 0) {
                     cand[nc++] = -c - 1;
                 } else if (next < 0) {
@@ -476,7 +490,7 @@ __global__ void __launch_bounds__(TRAV_THREADS) k_traverse(Dev<R> d) {
             }
         }
         qn += __shfl_sync(0xffffffffu, incl, 31);
-        __syncwarp();
+        __syncwarp();  // also: every lane has read its record row before the next load fills it
         const bool drain = !more && !__any_sync(0xffffffffu, walking);
         while (qn >= 32 || (drain && qn > 0)) {
             const int m = min(qn, 32);
@@ -586,8 +600,9 @@ __device__ __forceinline__ void sort_list(const Dev<R>& d, int k, int n) {
 // in the Newton iteration); with sortLists = 0 the lists are kept (substeps without detection,
 // collision.cu:121-172).  Then the lists of all vertices are packed in vertex order (csrOff,
 // csrCols): a tile takes its index from a ticket counter, scans its counts and resolves its
-// first slot by decoupled look-back over the tiles before it (which hold smaller tickets, so
-// they are running or done; each wait is bounded and a timeout sets IE_LIST_WAIT).  The tile's
+// first slot by decoupled look-back over the tiles before it, 32 at a time (they hold smaller
+// tickets, so they are running or done; each wait is bounded and a timeout sets
+// IE_LIST_WAIT).  The tile's
 // contacts are then evaluated 128 at a time, one per thread: the packed partner id, the
 // partner endpoints staged relative to p0 in the same slot, and the step-size limit
 // (collision.cu:121-159), of which each segment takes the minimum over its contacts in list
@@ -662,32 +677,50 @@ __global__ void __launch_bounds__(LIST_THREADS) k_lists(Dev<R> d, int sortLists)
     sScene[t] = sc;
     sA0[0][t] = a0.x; sA0[1][t] = a0.y; sA0[2][t] = a0.z;
     sA1[0][t] = a1.x; sA1[1][t] = a1.y; sA1[2][t] = a1.z;
-    // first packed slot of this tile: decoupled look-back (thread 0)
-    if (t == 0) {
+    // first packed slot of this tile: decoupled look-back by warp 0, 32 predecessors at a time
+    // (lane l reads tile hi - l; the window ends at the nearest tile that holds a prefix)
+    if (t < 32) {
+        const unsigned FULL = 0xffffffffu;
         const unsigned long long agg = (unsigned long long)sOff[B];
         unsigned long long excl = 0;
+        bool timedOut = false;
         if (tile > 0) {
-            bool timedOut = false;
-            for (int p = tile - 1; p >= 0; p--) {
-                unsigned long long w = st[p];
-                int spins = 0;
-                while ((w >> 62) == 0ull) {
-                    if (++spins > LIST_SPIN_LIMIT) {
-                        timedOut = true;
-                        break;
-                    }
-                    if (spins > 64) __nanosleep(32);
+            for (int hi = tile - 1; hi >= 0; hi -= 32) {
+                const int p = hi - t;
+                unsigned long long w = LS_PRE;  // before tile 0: an inclusive prefix of 0
+                if (p >= 0) {
                     w = st[p];
+                    int spins = 0;
+                    while ((w >> 62) == 0ull) {
+                        if (++spins > LIST_SPIN_LIMIT) {
+                            timedOut = true;
+                            break;
+                        }
+                        if (spins > 64) __nanosleep(32);
+                        w = st[p];
+                    }
                 }
-                if (timedOut) break;
-                excl += w & LS_VAL;
-                if (w & LS_PRE) break;
+                if (__any_sync(FULL, timedOut)) {
+                    timedOut = true;
+                    break;
+                }
+                const unsigned pre = __ballot_sync(FULL, (w & LS_PRE) != 0ull);
+                const int stop = pre ? __ffs(pre) - 1 : 31;
+                unsigned long long v = t <= stop ? (w & LS_VAL) : 0ull;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+                excl += v;
+                if (pre) break;
             }
-            if (timedOut) atomicOr(&d.err[EW_INTERNAL], IE_LIST_WAIT);
-            st[tile] = LS_PRE | (excl + agg);
+            if (t == 0) {
+                if (timedOut) atomicOr(&d.err[EW_INTERNAL], IE_LIST_WAIT);
+                st[tile] = LS_PRE | (excl + agg);
+            }
         }
-        if (excl + agg > (unsigned long long)d.csrCap) atomicOr(&d.err[EW_INTERNAL], IE_CONTACT);
-        sBase = excl;
+        if (t == 0) {
+            if (excl + agg > (unsigned long long)d.csrCap) atomicOr(&d.err[EW_INTERNAL], IE_CONTACT);
+            sBase = excl;
+        }
     }
     __syncthreads();
     const unsigned long long base = sBase;
@@ -825,10 +858,11 @@ __global__ void __launch_bounds__(TRAV_THREADS) k_traverse_packet(Dev<R> d) {
                 int next = -1;
 #pragma unroll
                 for (int e = 0; e < 4; e++) {
-                    const bool hit = mine && w.last[e] > qi && qb.mn[0] <= w.mx[0][e] && w.mn[0][e] <= qb.mx[0] &&
-                                     qb.mn[1] <= w.mx[1][e] && w.mn[1][e] <= qb.mx[1] && qb.mn[2] <= w.mx[2][e] &&
-                                     w.mn[2][e] <= qb.mx[2];
-                    const int c = w.code[e];  // the same in every lane
+                    const WEntry<R>& x = w.e[e];
+                    const bool hit = mine && x.last > qi && qb.mn[0] <= x.mx[0] && x.mn[0] <= qb.mx[0] &&
+                                     qb.mn[1] <= x.mx[1] && x.mn[1] <= qb.mx[1] && qb.mn[2] <= x.mx[2] &&
+                                     x.mn[2] <= qb.mx[2];
+                    const int c = x.code;  // the same in every lane
                     if (c < 0) {
                         if (hit) cand[nc++] = -c - 1;
                     } else if (__any_sync(FULL, hit)) {
