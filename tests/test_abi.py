@@ -105,3 +105,22 @@ def test_batch_scenes_must_share_a_schedule():
             s.configure()
         assert s._lib.yb_configure(s._h, ctypes.c_float(1e-3)) == 1  # YB_ERR_INVALID_ARGUMENT
         s.close()
+
+
+def test_walk_mode_and_small_path_switches():
+    """Broadphase walk modes 0 (per query), 1 (per warp of 32 queries) and 2 (per query with
+    cooperative record loads, the default) are accepted, other values refused; the
+    small-simulation switch takes 0 or 1.  No device work is needed to set them."""
+    lib = _abi.load()
+    h = ctypes.c_void_p()
+    assert lib.yb_create(64, ctypes.byref(h)) == 0
+    mode = ctypes.c_int32()
+    assert lib.yb_get_traversal(h, ctypes.byref(mode)) == 0 and mode.value == 2
+    for m in (0, 1, 2):
+        assert lib.yb_set_traversal(h, m) == 0
+        assert lib.yb_get_traversal(h, ctypes.byref(mode)) == 0 and mode.value == m
+    for m in (-1, 3):
+        assert lib.yb_set_traversal(h, m) == 1  # YB_ERR_INVALID_ARGUMENT
+    assert lib.yb_set_small_path(h, 0) == 0 and lib.yb_set_small_path(h, 1) == 0
+    assert lib.yb_set_small_path(h, 2) == 1
+    lib.yb_destroy(h)
