@@ -970,7 +970,10 @@ void launch_traverse(const Dev<R>& d, cudaStream_t s) {
 
 template <typename R>
 void launch_lists_step_limit(const Dev<R>& d, cudaStream_t s) {
-    if (d.nseg <= 0) return;
+    if (d.nseg <= 0) {  // no segment, no contact: the packed lists are empty
+        if (d.n > 0) cudaMemsetAsync(d.csrOff, 0, sizeof(unsigned) * (d.n + 1), s);
+        return;
+    }
     launch_lists(d, 0, s);
 }
 
