@@ -488,15 +488,31 @@ def run_serve(args):
     frames run (the frame thread makes every CUDA call).
     Arrivals stop after the window; the requests already in the batch then finish (no new
     admissions, at most --drain seconds) and the rest of the queue is reported as not served.
-    Beside it, a sample of the same requests served one at a time through plain advance()."""
+    Beside it, a sample of the same requests served one at a time through plain advance().
+    Under torchrun every rank runs its own server on its GPU and takes every world-th request of
+    the one arrival stream (sharding.route_requests); no collective on the data path, rank 0
+    gathers the reports and prints the job's line."""
     import torch
 
-    from yarnball_b200 import serve
+    from yarnball_b200 import serve, sharding
 
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    reqs = serve.poisson_requests(args.rate, args.duration, frames=args.frames)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    all_reqs = serve.poisson_requests(args.rate, args.duration, frames=args.frames)
+    mine = set(sharding.route_requests([r.id for r in all_reqs], world, rank))
+    reqs = [r for r in all_reqs if r.id in mine]
     server = serve.Server(budget_bytes=args.budget_gb * 1e9, shape=(128, 0), stream=torch.cuda.Stream(),
                           setup_threads=args.setup_threads, max_batch_vertices=args.max_batch_verts or None)
+    if dist:
+        dist.barrier()
     pending = list(reqs)
     t0 = time.perf_counter()
     while True:
@@ -518,56 +534,83 @@ def run_serve(args):
             if r.finished_at is None:
                 r.finished_at = done_t
     wall = time.perf_counter() - t0
-    served_work = float(sum(server.frame_sizes)) * SUBSTEPS  # vertex-substeps advanced
     arrived = [r for r in reqs if r.arrival <= min(wall, args.duration)]
     done = [r for r in reqs if r.finished_at is not None]
-    lat = [r.finished_at - r.arrival for r in done]
-    wait = [r.admitted_at - r.arrival for r in done]
-    work = sum(r.vertices * SUBSTEPS * r.frames for r in done)
-    dev_s = sum(server.frame_ms) / 1e3
-    mean_req_work = float(np.mean([r.vertices * SUBSTEPS * r.frames for r in arrived])) if arrived else 0.0
-    queue_end = len(server.queue)
-    server.close()
-    # a sample of the same requests, each alone through plain advance(), one after the other
-    sample = arrived[: args.alone_sample]
-    service = []
-    for r in sample:
-        sim = serve.build_request_sim(r, (128, 0))
-        st = torch.cuda.Stream()
-        sim.set_stream(st.cuda_stream)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(st)
-        for _ in range(r.frames):
-            sim.advance(FRAME)
-        e1.record(st)
-        e1.synchronize()
-        service.append(e0.elapsed_time(e1) / 1e3)
-        sim.close()
-    alone_tp = sum(r.vertices * SUBSTEPS * r.frames for r in sample) / max(sum(service), 1e-9)
-    batched_tp = served_work / max(wall, 1e-9)
-    out = {
-        "metric": "serving: request latency and vertex-substeps/s under Poisson arrivals", "unit": "s",
-        "rate_per_s": args.rate, "arrival_window_s": args.duration, "frames_per_request": args.frames,
-        "budget_gb": args.budget_gb, "max_batch_vertices": args.max_batch_verts or None,
-        "setup_threads": args.setup_threads,
-        "requests": {"arrived": len(arrived), "admitted": sum(1 for r in reqs if r.admitted_at is not None),
-                     "completed": len(done), "queued_at_end": queue_end},
-        "request_latency_s": serve.percentiles(lat), "queue_wait_s": serve.percentiles(wait),
-        "frame_latency_ms": serve.percentiles(server.frame_ms), "frames": len(server.frame_ms),
-        "batch_vertices": serve.percentiles([float(x) for x in server.frame_sizes]),
-        "queue_length": {"max": max(server.queue_lengths) if server.queue_lengths else 0, "end": queue_end},
-        "gathers": server.gathers,
-        "throughput_vertex_substeps_per_s": batched_tp,
-        "device_throughput_vertex_substeps_per_s": served_work / max(dev_s, 1e-9),
-        "completed_work_vertex_substeps": work, "wall_s": wall,
-        "offered_load_vertex_substeps_per_s": mean_req_work * args.rate,
-        "sustainable_rate_per_s": batched_tp / mean_req_work if mean_req_work else None,
-        "alone": {"requests": len(sample), "throughput_vertex_substeps_per_s": alone_tp,
-                  "service_s": serve.percentiles(service)},
-        "batched_over_alone": batched_tp / alone_tp if alone_tp else None,
-        "request_vertices": serve.percentiles([r.vertices for r in arrived]),
+    report = {
+        "wall": wall, "served_work": float(sum(server.frame_sizes)) * SUBSTEPS,  # vertex-substeps advanced
+        "dev_s": sum(server.frame_ms) / 1e3,
+        "arrived_work": [r.vertices * SUBSTEPS * r.frames for r in arrived],
+        "arrived_vertices": [r.vertices for r in arrived],
+        "admitted": sum(1 for r in reqs if r.admitted_at is not None), "completed": len(done),
+        "work": sum(r.vertices * SUBSTEPS * r.frames for r in done),
+        "lat": [r.finished_at - r.arrival for r in done], "wait": [r.admitted_at - r.arrival for r in done],
+        "frame_ms": list(server.frame_ms), "admit_ms": list(server.admit_ms), "gather_ms": list(server.gather_ms),
+        "frame_sizes": [float(x) for x in server.frame_sizes], "queue_end": len(server.queue),
+        "queue_max": max(server.queue_lengths) if server.queue_lengths else 0, "gathers": server.gathers,
     }
-    print(json.dumps(out))
+    server.close()
+    reports = sharding.gather_to_rank0(report)
+    if rank == 0:
+        # a sample of rank 0's requests, each alone through plain advance(), one after the other
+        sample = arrived[: args.alone_sample]
+        service = []
+        for r in sample:
+            sim = serve.build_request_sim(r, (128, 0))
+            st = torch.cuda.Stream()
+            sim.set_stream(st.cuda_stream)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(r.frames):
+                sim.advance(FRAME)
+            e1.record(st)
+            e1.synchronize()
+            service.append(e0.elapsed_time(e1) / 1e3)
+            sim.close()
+        alone_tp = sum(r.vertices * SUBSTEPS * r.frames for r in sample) / max(sum(service), 1e-9)
+
+        def cat(key):
+            return [x for rep in reports for x in rep[key]]
+
+        wall_max = max(rep["wall"] for rep in reports)
+        served_work = sum(rep["served_work"] for rep in reports)
+        dev_s = max(rep["dev_s"] for rep in reports)
+        arrived_work = cat("arrived_work")
+        mean_req_work = float(np.mean(arrived_work)) if arrived_work else 0.0
+        batched_tp = served_work / max(wall_max, 1e-9)
+        queue_end = sum(rep["queue_end"] for rep in reports)
+        out = {
+            "metric": "serving: request latency and vertex-substeps/s under Poisson arrivals", "unit": "s",
+            "n_gpus": world, "rate_per_s": args.rate, "arrival_window_s": args.duration,
+            "frames_per_request": args.frames, "budget_gb": args.budget_gb,
+            "max_batch_vertices": args.max_batch_verts or None, "setup_threads": args.setup_threads,
+            "routing": "one server per GPU, request i on rank i mod %d" % world,
+            "requests": {"arrived": len(arrived_work), "admitted": sum(rep["admitted"] for rep in reports),
+                         "completed": sum(rep["completed"] for rep in reports), "queued_at_end": queue_end},
+            "request_latency_s": serve.percentiles(cat("lat")), "queue_wait_s": serve.percentiles(cat("wait")),
+            "frame_latency_ms": serve.percentiles(cat("frame_ms")), "frames": len(cat("frame_ms")),
+            "frame_boundary_ms": {"admission_host": serve.percentiles(cat("admit_ms")),
+                                  "regather_host": serve.percentiles(cat("gather_ms")),
+                                  "what": "host time at each frame boundary before the frame's advance: building "
+                                          "the admitted requests as one-scene Sims (configure, upload) and "
+                                          "re-gathering the batch (yb_batch_gather device copies included); "
+                                          "frame_latency_ms is the device time of the advance"},
+            "batch_vertices": serve.percentiles(cat("frame_sizes")),
+            "queue_length": {"max": max(rep["queue_max"] for rep in reports), "end": queue_end},
+            "gathers": sum(rep["gathers"] for rep in reports),
+            "throughput_vertex_substeps_per_s": batched_tp,
+            "device_throughput_vertex_substeps_per_s": served_work / max(dev_s, 1e-9),
+            "completed_work_vertex_substeps": sum(rep["work"] for rep in reports), "wall_s": wall_max,
+            "offered_load_vertex_substeps_per_s": mean_req_work * args.rate,
+            "sustainable_rate_per_s": batched_tp / mean_req_work if mean_req_work else None,
+            "alone": {"requests": len(sample), "throughput_vertex_substeps_per_s": alone_tp,
+                      "service_s": serve.percentiles(service)},
+            "batched_over_alone": (batched_tp / world) / alone_tp if alone_tp else None,
+            "request_vertices": serve.percentiles(cat("arrived_vertices")),
+        }
+        print(json.dumps(out))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def run_twist(args):

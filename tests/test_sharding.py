@@ -1,5 +1,6 @@
-"""Multi-rank logic on CPU: two gloo ranks partition the batched workload's scenes and reduce
-timings the way bench.py does on GPUs (no GPU involved)."""
+"""Multi-rank logic on CPU: two gloo ranks partition the batched workload's scenes, reduce
+timings, route serving requests and gather their reports the way bench.py does on GPUs (no GPU
+involved)."""
 import os
 import socket
 
@@ -30,7 +31,9 @@ def _worker(rank, world, port, sizes, out):
     verts = int(sum(sizes[i] for i in mine))
     ms, total = sharding.reduce_timing(10.0 + rank, verts)
     stats = sharding.reduce_stats([1.0, float(verts)])
-    out[rank] = (mine, ms, total, stats.tolist())
+    routed = sharding.route_requests(list(range(101)), world, rank)
+    gathered = sharding.gather_to_rank0({"rank": rank, "requests": routed})
+    out[rank] = (mine, ms, total, stats.tolist(), routed, gathered)
     dist.barrier()
     dist.destroy_process_group()
 
@@ -59,13 +62,18 @@ def test_two_gloo_ranks_agree_on_partition_and_reduce():
         res = dict(out)
     parts = sharding.partition_scenes(sizes, world)
     for r in range(world):
-        mine, ms, total, stats = res[r]
+        mine, ms, total, stats, routed, gathered = res[r]
         assert mine == parts[r]
         assert ms == 11.0  # max over ranks
         assert total == float(sum(sizes))
         assert stats[0] == 2.0 and stats[1] == float(sum(sizes))
     assert sorted(res[0][0] + res[1][0]) == list(range(len(sizes)))
     np.testing.assert_equal(len(set(res[0][0]) & set(res[1][0])), 0)
+    # serving: each request goes to exactly one rank; rank 0 receives every rank's report
+    assert sorted(res[0][4] + res[1][4]) == list(range(101))
+    assert abs(len(res[0][4]) - len(res[1][4])) <= 1
+    assert [g["rank"] for g in res[0][5]] == [0, 1] and res[0][5][1]["requests"] == res[1][4]
+    assert res[1][5] is None
 
 
 def test_rank_subsets_hold_the_one_gpu_geometry():

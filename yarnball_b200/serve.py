@@ -26,6 +26,7 @@ the multi-block kernels to rounding.
 """
 import collections
 import math
+import time
 from concurrent.futures import Future, ThreadPoolExecutor
 
 import numpy as np
@@ -116,6 +117,8 @@ class Server:
         self.spare = None
         self.finished = []
         self.frame_ms = []            # device time of each batched frame
+        self.admit_ms = []            # host time of each frame boundary's admissions (one-scene Sims built)
+        self.gather_ms = []           # host time of each re-gather (device copies included, 0 without one)
         self.frame_sizes = []         # vertices advanced in each frame
         self.queue_lengths = []       # queued requests at each frame boundary
         self.gathers = 0
@@ -215,13 +218,18 @@ class Server:
             self.queue[0].future.result()  # an idle server waits for its next request
         self.queue_lengths.append(len(self.queue))
         keep = [i for i, r in enumerate(self.active) if r.done_frames < r.frames]
+        t0 = time.perf_counter()
         joined = self._admit() if admit else []
+        t1 = time.perf_counter()
         for r in joined:
             r.admitted_at = now
         if len(keep) != len(self.active) or joined:
             self._regather(keep, joined)
+        t2 = time.perf_counter()
         if not self.active:
             return 0.0
+        self.admit_ms.append((t1 - t0) * 1e3)
+        self.gather_ms.append((t2 - t1) * 1e3)
         import torch
 
         if self.stream is None:  # the batch must run on the stream the events are recorded on

@@ -57,3 +57,22 @@ def reduce_stats(values, device=None):
     t = torch.tensor(v, dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return t.cpu().numpy()
+
+
+def route_requests(request_ids, world, rank):
+    """Requests of a serving stream handled by `rank` of `world` GPUs, each running its own
+    server: round-robin on the request id (arrival order), so every rank sees the same arrival
+    process thinned by `world` and each request goes to exactly one rank."""
+    return [i for i in request_ids if i % world == rank]
+
+
+def gather_to_rank0(obj):
+    """Every rank's object, gathered on rank 0 (a list in rank order; None elsewhere); without a
+    process group the object alone, as a one-element list."""
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()):
+        return [obj]
+    out = [None] * dist.get_world_size() if dist.get_rank() == 0 else None
+    dist.gather_object(obj, out, dst=0)
+    return out
