@@ -80,7 +80,8 @@ def workload_desc(spec):
         "substeps_per_step": SUBSTEPS,
         "newton_iterations": NUM_ITR,
         "step": "advance(1/30 s) of the whole batch (%d substeps of h=1/%d s)" % (SUBSTEPS, SUBSTEPS * 30),
-        "l2": "inputs larger than L2 (state ~0.8 KB/vertex x %.1fM vertices), no flush" % (n / 1e6),
+        "l2": "inputs larger than L2 (one Newton iteration alone moves ~260 B of DRAM traffic per vertex, "
+              "%.1f GB for %.1fM vertices, against 126 MB of L2), no flush" % (n * 260e-9, n / 1e6),
         "seed": SEED,
         "parallelism": "one GPU",
     }
