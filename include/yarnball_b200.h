@@ -372,6 +372,10 @@ yb_status yb_debug_contacts(yb_sim* sim, int32_t* numCols, int32_t* cols, float*
 yb_status yb_debug_dx(yb_sim* sim, double* dx4);
 /* Velocity of the previous substep (the predictor's lastVels, iteration.cu:19-20), 3n doubles. */
 yb_status yb_debug_last_vel(yb_sim* sim, double* lastVel3);
+/* The contact lists packed in vertex order by the last list pass (what the Newton kernels read):
+ * offsets (n + 1 uint32; vertex k's partners are cols[offsets[k] .. offsets[k+1])), then up to
+ * capacity partner ids into cols. */
+yb_status yb_debug_packed_contacts(yb_sim* sim, uint32_t* offsets, int32_t* cols, int64_t capacity);
 
 /* Runs only the substep phases selected by mask on the current device state:
  * 1 = predictor (initItr), 2 = detection with BVH rebuild, 4 = detection with refit only,

@@ -282,3 +282,27 @@ def test_packet_and_per_query_traversal_give_the_same_lists(which):
         sim.close()
         orc.close()
     assert np.array_equal(out[1][0], out[0][0]) and np.array_equal(out[1][0], out[2][0])
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_packed_lists_equal_the_sorted_rows(precision):
+    """The list pass packs every vertex's sorted contact row into consecutive slots in vertex
+    order (what the Newton kernels read): the offsets are the running sum of the list lengths,
+    each vertex's slots hold exactly its sorted row, after a detection on a refitted tree and
+    after a list pass without detection."""
+    spec = scenes.batched_spec(seed=7, num_scenes=24, cap=1500000)
+    sim = scenes.build_batched(seed=7, spec=spec, precision=precision)[0]
+    sim.advance(FRAME)
+    for mask in (1 | 4, 8):
+        sim.debug_phases(mask, H)
+        nc, rows, _ = sim.debug_contacts(raw=True)
+        off, cols = sim.debug_packed_contacts()
+        assert off[0] == 0 and np.all(np.diff(off.astype(np.int64)) == nc)
+        assert int(off[-1]) == int(nc.sum()) > 0
+        with_c = np.nonzero(nc)[0]
+        assert np.array_equal(cols, np.concatenate([rows[k] for k in with_c]))
+        # each row ascending (the list pass sorted it): every step inside a row increases
+        inside = np.ones(len(cols), bool)
+        inside[off[with_c].astype(np.int64)] = False
+        assert np.all(np.diff(cols.astype(np.int64))[inside[1:]] > 0)
+    sim.close()

@@ -145,6 +145,7 @@ SIGNATURES = {
     "yb_debug_contacts": (ctypes.c_int, [_P, c_int32_p, c_int32_p, c_float_p]),
     "yb_debug_dx": (ctypes.c_int, [_P, c_double_p]),
     "yb_debug_last_vel": (ctypes.c_int, [_P, c_double_p]),
+    "yb_debug_packed_contacts": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint32), c_int32_p, ctypes.c_int64]),
     "yb_set_traversal": (ctypes.c_int, [_P, ctypes.c_int32]),
     "yb_set_small_path": (ctypes.c_int, [_P, ctypes.c_int32]),
     "yb_get_traversal": (ctypes.c_int, [_P, c_int32_p]),

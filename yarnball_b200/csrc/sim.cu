@@ -67,6 +67,7 @@ struct EngineBase {
     virtual void set_traversal(int packet) = 0;
     virtual bool small_fits() const = 0;
     virtual yb_status run_small(int steps) = 0;
+    virtual yb_status packed_contacts(uint32_t* off, int32_t* cols, int64_t capacity) = 0;
 };
 
 }  // namespace
@@ -863,6 +864,22 @@ struct Engine : EngineBase {
             out[3 * i] = (double)h[i].x;
             out[3 * i + 1] = (double)h[i].y;
             out[3 * i + 2] = (double)h[i].z;
+        }
+        return YB_OK;
+    }
+
+    // The packed lists the Newton kernels read: n + 1 offsets, then up to capacity partner ids.
+    yb_status packed_contacts(uint32_t* off, int32_t* cols, int64_t capacity) override {
+        const size_t n = (size_t)S->n;
+        cudaStream_t st = S->stream;
+        std::vector<uint32_t> o(n + 1);
+        YB_CUDA(cudaMemcpyAsync(o.data(), d.csrOff, sizeof(uint32_t) * (n + 1), cudaMemcpyDeviceToHost, st));
+        YB_CUDA(cudaStreamSynchronize(st));
+        if (off) std::memcpy(off, o.data(), sizeof(uint32_t) * (n + 1));
+        const size_t total = std::min((size_t)o[n], (size_t)std::max<int64_t>(capacity, 0));
+        if (cols && total) {
+            YB_CUDA(cudaMemcpyAsync(cols, d.csrCols, sizeof(int32_t) * total, cudaMemcpyDeviceToHost, st));
+            YB_CUDA(cudaStreamSynchronize(st));
         }
         return YB_OK;
     }
@@ -1859,6 +1876,12 @@ yb_status yb_debug_contacts(yb_sim* S, int32_t* numCols, int32_t* cols, float* s
     if (!S) return YB_ERR_INVALID_ARGUMENT;
     if (!S->configured) return YB_ERR_NOT_CONFIGURED;
     return S->eng->contacts(numCols, cols, stepLimit);
+}
+
+yb_status yb_debug_packed_contacts(yb_sim* S, uint32_t* offsets, int32_t* cols, int64_t capacity) {
+    if (!S || !offsets || capacity < 0 || (capacity > 0 && !cols)) return YB_ERR_INVALID_ARGUMENT;
+    if (!S->configured) return YB_ERR_NOT_CONFIGURED;
+    return S->eng->packed_contacts(offsets, cols, capacity);
 }
 
 yb_status yb_debug_last_vel(yb_sim* S, double* lastVel3) {

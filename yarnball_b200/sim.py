@@ -392,6 +392,15 @@ class Sim:
         m = (1 if mode else 0) if isinstance(mode, bool) else int(mode)
         check(self._lib.yb_set_traversal(self._h, m), "traversal")
 
+    def debug_packed_contacts(self):
+        """(offsets, cols): the vertex-ordered packed lists of the last list pass."""
+        off = np.zeros(self.numVerts + 1, np.uint32)
+        check(self._lib.yb_debug_packed_contacts(self._h, ptr(off, ctypes.c_uint32), None, 0), "packed")
+        cols = np.zeros(max(int(off[-1]), 1), np.int32)
+        check(self._lib.yb_debug_packed_contacts(self._h, ptr(off, ctypes.c_uint32), ptr(cols, ctypes.c_int32),
+                                                 int(off[-1])), "packed")
+        return off, cols[:int(off[-1])]
+
     def debug_last_vel(self):
         lv = np.zeros((self.numVerts, 3))
         check(self._lib.yb_debug_last_vel(self._h, ptr(lv, ctypes.c_double)), "lastVel")
