@@ -397,11 +397,12 @@ yb_status yb_debug_sort_pairs(const uint64_t* keys, const int32_t* vals, int32_t
  * sort is never in place); stream is a cudaStream_t (NULL = legacy default).  Scratch is a fixed
  * array compiled into the library (about 4.2 MB held on every GPU that loads it), so n is
  * limited to YB_SORT_NOALLOC_MAX_N; larger n returns YB_ERR_SCRATCH_TOO_SMALL.  No
- * cudaMalloc/cudaFree or allocating library call is made.  The first call on a device looks
- * the scratch address up (make it before any stream capture) and keeps it for the life of the
- * process (do not reset the device while the library is in use).  Calls share the scratch:
- * calls that overlap on the GPU race and must be serialised.  Returns after the sort has
- * completed on `stream`. */
+ * cudaMalloc/cudaFree or allocating library call is made; under lazy module loading the first
+ * call on a device loads the library's kernels and the scratch array there (once), so make
+ * that first call where loading is allowed.  Each call synchronises `stream` (it reads back an
+ * error word), so it cannot be captured in a CUDA graph.  Calls share the scratch: calls that
+ * overlap on the GPU race and must be serialised.  Returns after the sort has completed on
+ * `stream`. */
 #define YB_SORT_NOALLOC_MAX_N 262144
 yb_status yb_sort_pairs_noalloc(const uint64_t* keysIn, const int32_t* valsIn, uint64_t* keysOut,
                                 int32_t* valsOut, int32_t n, int32_t bits, void* stream);

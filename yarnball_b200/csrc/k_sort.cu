@@ -10,7 +10,6 @@
 // Tiles only wait on tiles that obtained a smaller index from the counter, i.e. that are
 // already running, so the look-back always completes; every wait is still bounded and a
 // timeout sets IE_SORT_WAIT in the error word instead of hanging.
-#include <mutex>
 
 #include "engine.cuh"
 #include "yarnball_b200.h"
@@ -198,13 +197,13 @@ int radix_sort_pairs(unsigned long long* keys[2], int* vals[2], int n, int bits,
 // the device, or fail once memory is fragmented) is treated as an error.  This variant uses
 // only the caller's input/output buffers plus one fixed scratch area compiled into the
 // library as a file-scope __device__ array.  Every GPU that loads the library holds that
-// array (about 4.2 MB) until the process exits.  The library looks its address up once per
-// device with cudaGetSymbolAddress (host code may not use the symbol itself as a device
-// address); that set-up happens inside the first call on each device, so make that first
-// call before any stream capture.  The looked-up address is kept for the life of the process,
-// so the device may not be reset (cudaDeviceReset) while the library is in use.  All calls
-// share the array: calls whose GPU work overlaps (two streams, or two host threads at once)
-// race on it and must be serialised by the caller.
+// array (about 4.2 MB) until the process exits.  Each call looks its address up with
+// cudaGetSymbolAddress (host code may not use the symbol itself as a device address).  With
+// lazy module loading the first call on a device loads the library's kernels and this array
+// there, once; later calls allocate nothing.  Each call reads back an error word and
+// synchronises its stream, so it cannot be captured in a CUDA graph.  All calls share the
+// array: calls whose GPU work overlaps (two streams, or two host threads at once) race on it
+// and must be serialised by the caller.
 namespace yb {
 namespace {
 
@@ -221,24 +220,13 @@ struct NoAllocScratch {
 
 static __device__ __align__(256) unsigned char g_sort_scratch[sizeof(NoAllocScratch)];
 
-constexpr int MAX_DEVICES = 256;
-std::mutex g_scratch_mu;
-void* g_scratch_addr[MAX_DEVICES] = {nullptr};
-
-// Device address of g_sort_scratch on the current device (looked up once per device).
+// Device address of g_sort_scratch in the current context, looked up on every call (a
+// driver table lookup), so no address outlives a device reset.
 cudaError_t scratch_address(NoAllocScratch** out) {
-    int dev = -1;
-    cudaError_t e = cudaGetDevice(&dev);
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_sort_scratch);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= MAX_DEVICES) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_sort_scratch);
-        if (e != cudaSuccess) return e;
-        g_scratch_addr[dev] = p;
-    }
-    *out = (NoAllocScratch*)g_scratch_addr[dev];
+    *out = (NoAllocScratch*)p;
     return cudaSuccess;
 }
 
