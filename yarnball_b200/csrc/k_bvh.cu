@@ -316,6 +316,7 @@ constexpr int BVH_STACK = 96;
 constexpr int TRAV_THREADS = 128;
 constexpr int TRAV_WARPS = TRAV_THREADS / 32;
 constexpr int TRAV_QCAP = 160;      // < 32 left over + up to 4 candidates per lane
+constexpr int TRAV_GRAB = 32;       // queries a warp takes from the counter at a time
 
 // Appends y to x's contact list.  The count keeps growing past MAX_COLS so that the list
 // kernel can report the overflow (collision.cu:80-90).
@@ -331,9 +332,10 @@ __device__ __forceinline__ void list_append(const Dev<R>& d, int x, int y) {
 // the one with the lower sorted position, whose walk skips every entry holding only leaves at
 // or before its own position.  The walk runs over the wide nodes (four grandchildren per
 // node), so a query takes half as many dependent node loads as on the binary tree.  Lanes walk
-// independently, with a per-lane stack; a lane that finishes takes the next unprocessed query
-// from a global counter (one atomic per warp and refill), so a warp keeps all 32 lanes busy
-// until the queries run out (persistent grid).  A leaf entry that overlaps a lane's box
+// independently, with a per-lane stack; a lane that finishes takes the next query of its
+// warp's range of TRAV_GRAB queries (ranges come from a global counter, the next one requested
+// while the current one is used), so a warp keeps all 32 lanes busy until the queries run out
+// (persistent grid) with one atomic per TRAV_GRAB queries.  A leaf entry that overlaps a lane's box
 // becomes a candidate pair in a per-warp queue; whenever 32 candidates are queued the warp
 // runs the separately rounded narrow-phase test on them, one pair per lane, with the lower
 // segment index as segment A, and appends kept pairs to both lists.  The pair set is the same
@@ -402,16 +404,27 @@ __global__ void __launch_bounds__(TRAV_THREADS) k_traverse(Dev<R> d) {
     Box<R> qb;
     int qn = 0;        // queued candidates (identical in every lane)
     bool more = true;  // the counter has not run out (warp-uniform)
+    // Queries are handed out TRAV_GRAB at a time: the warp's current range [poolNext, poolEnd)
+    // and, in lane 0, the start of the next range, requested one range ahead so that a refill
+    // rarely waits on the counter.  Ranges come from one counter in increasing order, so a
+    // warp whose current range reaches nseg holds no later valid query.
+    int poolNext = 0, poolEnd = 0;
+    int pend = 0;
+    if (lane == 0) pend = (int)atomicAdd(d.travNext, (unsigned)TRAV_GRAB);
     while (true) {
         // Refill lanes without a walk.
         const unsigned idle = __ballot_sync(0xffffffffu, !walking);
         if (more && idle) {
-            int base = 0;
-            if (lane == 0) base = (int)atomicAdd(d.travNext, (unsigned)__popc(idle));
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (base + __popc(idle) >= nseg) more = false;
+            const int need = __popc(idle);  // <= 32 <= TRAV_GRAB: at most one new range
+            const int avail = poolEnd - poolNext;
+            int next = 0;
+            if (avail < need) {
+                next = __shfl_sync(0xffffffffu, pend, 0);
+                if (lane == 0) pend = (int)atomicAdd(d.travNext, (unsigned)TRAV_GRAB);
+            }
             if (!walking) {
-                qi = base + __popc(idle & lt);
+                const int rank = __popc(idle & lt);
+                qi = rank < avail ? poolNext + rank : next + (rank - avail);
                 if (qi < nseg) {
                     QRec<R> r;
                     if constexpr (sizeof(R) == 4) {
@@ -435,6 +448,13 @@ __global__ void __launch_bounds__(TRAV_THREADS) k_traverse(Dev<R> d) {
                     walking = node >= 0 && d.sceneLast[sc] > qi;  // a leaf root has no pairs
                 }
             }
+            if (avail >= need) {
+                poolNext += need;
+            } else {
+                poolNext = next + (need - avail);
+                poolEnd = next + TRAV_GRAB;
+            }
+            if (poolNext >= nseg) more = false;
         }
         if (!more && !__any_sync(0xffffffffu, walking) && qn == 0) break;
         int cand[4];
